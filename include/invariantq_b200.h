@@ -1,0 +1,166 @@
+/*
+ * invariantq_b200.h -- C ABI of libinvariantq.so, the B200 (sm_100a) CUDA
+ * implementation of InvariantQ's state-vector and density-matrix core.
+ *
+ * Part 1 repeats, symbol for symbol and with the same signatures, the
+ * reference's C ABI (core/include/c_api.h:10-65) that its ctypes binding
+ * (invariantq/core/binding.py:54-299) binds at import time, so this library
+ * drops in under the unmodified binding.  Each declaration names the reference
+ * function it replaces.  Part 2 adds entry points the reference does not have.
+ *
+ * Conventions (as the reference): qubit q is bit q of the amplitude index;
+ * matrices are row-major with split real/imaginary double arrays; a 2-qubit
+ * matrix's local index has q0 as its most significant bit; a fused k-qubit
+ * matrix (k >= 3) has qubits[b] as local index bit b.  A density matrix is
+ * row-major rho[r * 2^n + c].
+ *
+ * Execution model: amplitudes live in GPU memory.  Gate and channel calls are
+ * queued on the handle and applied in fused tile passes when a result is read
+ * (or the queue is long); every call that returns data to the host waits for
+ * the GPU first, so the host-visible behaviour is that of the reference's
+ * synchronous calls.  Calls on one handle must not overlap; distinct handles
+ * are independent.
+ *
+ * Errors: where the reference throws through extern "C" (and so terminates the
+ * process) this library records a message (iq_last_error) and returns: void
+ * calls become no-ops, int calls return -1, double calls return NaN, create
+ * returns NULL.  NULL pointer arguments are silent no-ops returning 0, as in the
+ * reference (core/src/api.cpp).
+ */
+#ifndef INVARIANTQ_B200_H
+#define INVARIANTQ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===================== Part 1: the reference ABI (core/include/c_api.h) ===================== */
+
+/* -- state vector (c_api.h:11-24; implementations core/src/api.cpp:14-112) -- */
+void* iq_statevector_create(size_t num_qubits);                                   /* api.cpp:14-20  */
+void  iq_statevector_free(void* sv);                                              /* api.cpp:22-24  */
+void  iq_statevector_reset(void* sv);                                             /* api.cpp:26-28  */
+void  iq_statevector_apply_1q(void* sv, size_t target, const double* u_real,
+                              const double* u_imag);                              /* api.cpp:30-37, statevector.cpp:26-47 */
+void  iq_statevector_apply_2q(void* sv, size_t q0, size_t q1, const double* u_real,
+                              const double* u_imag);                              /* api.cpp:39-46, statevector.cpp:49-87 */
+void  iq_statevector_apply_fused(void* sv, const size_t* qubits, size_t k,
+                                 const double* u_real, const double* u_imag);     /* api.cpp:48-57, statevector.cpp:89-152; k <= 5 here (reference: 4) */
+int   iq_statevector_measure(void* sv, size_t target, double rand_val);           /* api.cpp:59-62, statevector.cpp:190-195 */
+void  iq_statevector_reset_qubit(void* sv, size_t target, double rand_val);       /* api.cpp:64-67, statevector.cpp:197-204 */
+double iq_statevector_measure_prob(void* sv, size_t target, int outcome);         /* api.cpp:69-72, statevector.cpp:154-169 */
+void  iq_statevector_get_amplitudes(void* sv, double* real_out, double* imag_out);/* api.cpp:74-83  */
+void  iq_statevector_get_probabilities(void* sv, double* probs_out);              /* api.cpp:85-90, statevector.cpp:226-233 */
+void  iq_statevector_sample(void* sv, size_t num_shots, uint64_t seed,
+                            uint64_t* results_out);                               /* api.cpp:92-97, statevector.cpp:235-256 */
+double iq_statevector_entropy(void* sv, const size_t* qubits, size_t num_subsys_qubits); /* api.cpp:99-103, statevector.cpp:293-410 */
+void  iq_statevector_expval_pauli(void* sv, const char* pauli_str, const size_t* qubits,
+                                  size_t len, double* val_real, double* val_imag);/* api.cpp:105-112, statevector.cpp:258-291 */
+
+/* -- density matrix (c_api.h:27-38; api.cpp:116-192) -- */
+void* iq_density_matrix_create(size_t num_qubits);                                /* api.cpp:116-122 */
+void  iq_density_matrix_free(void* dm);                                           /* api.cpp:124-126 */
+void  iq_density_matrix_reset(void* dm);                                          /* api.cpp:128-130 */
+void  iq_density_matrix_apply_1q_unitary(void* dm, size_t target, const double* u_real,
+                                         const double* u_imag);                   /* api.cpp:132-137, density_matrix.cpp:18-67 */
+void  iq_density_matrix_apply_2q_unitary(void* dm, size_t q0, size_t q1, const double* u_real,
+                                         const double* u_imag);                   /* api.cpp:139-144, density_matrix.cpp:69-145 */
+void  iq_density_matrix_apply_kraus_1q(void* dm, size_t target, size_t num_kraus,
+                                       const double* k_real, const double* k_imag);/* api.cpp:146-155, density_matrix.cpp:147-163 */
+void  iq_density_matrix_get_elements(void* dm, double* real_out, double* imag_out);/* api.cpp:157-167 */
+double iq_density_matrix_trace(void* dm);                                         /* api.cpp:169-172, density_matrix.cpp:193-199 */
+double iq_density_matrix_purity(void* dm);                                        /* api.cpp:174-177, density_matrix.cpp:201-208 */
+double iq_density_matrix_entropy(void* dm);                                       /* api.cpp:179-182, density_matrix.cpp:310-380 */
+int   iq_density_matrix_measure(void* dm, size_t target, double rand_val);        /* api.cpp:184-187, density_matrix.cpp:218-256 */
+void  iq_density_matrix_reset_qubit(void* dm, size_t target);                     /* api.cpp:189-192, density_matrix.cpp:258-269 */
+
+/* -- stabilizer (c_api.h:41-55) and MPS (c_api.h:58-65).  Not GPU paths: these
+ * forward to a CPU core named by the environment variable IQ_CPU_CORE_LIB (a
+ * build of the reference's core/ library) when it is set; otherwise create
+ * returns NULL with an error message and the other calls are no-ops. -- */
+void* iq_stabilizer_create(size_t num_qubits);
+void  iq_stabilizer_free(void* stab);
+void  iq_stabilizer_reset(void* stab);
+void  iq_stabilizer_reset_qubit(void* stab, size_t a, double rand_val);
+void  iq_stabilizer_apply_h(void* stab, size_t a);
+void  iq_stabilizer_apply_s(void* stab, size_t a);
+void  iq_stabilizer_apply_sdg(void* stab, size_t a);
+void  iq_stabilizer_apply_cnot(void* stab, size_t a, size_t b);
+void  iq_stabilizer_apply_cz(void* stab, size_t a, size_t b);
+void  iq_stabilizer_apply_swap(void* stab, size_t a, size_t b);
+void  iq_stabilizer_apply_x(void* stab, size_t a);
+void  iq_stabilizer_apply_y(void* stab, size_t a);
+void  iq_stabilizer_apply_z(void* stab, size_t a);
+int   iq_stabilizer_measure(void* stab, size_t a, double rand_val);
+void  iq_stabilizer_to_string(void* stab, char* buffer, size_t max_len);
+void* iq_mps_create(size_t num_qubits, size_t max_bond_dim, double cutoff);
+void  iq_mps_free(void* mps);
+void  iq_mps_reset(void* mps);
+void  iq_mps_apply_1q(void* mps, size_t target, const double* u_real, const double* u_imag);
+void  iq_mps_apply_2q(void* mps, size_t q0, size_t q1, const double* u_real, const double* u_imag);
+double iq_mps_entropy(void* mps, size_t bond_idx);
+void  iq_mps_to_statevector(void* mps, double* real_out, double* imag_out);
+int   iq_mps_measure(void* mps, size_t target, double rand_val);
+
+/* ===================== Part 2: additions (no counterpart in the reference) ===================== */
+
+/* Last error recorded on the calling thread: returns its code (0 = none) and
+ * copies the message (NUL-terminated, truncated to len). */
+int  iq_last_error(char* buf, size_t len);
+void iq_clear_error(void);
+const char* iq_version(void);
+/* Kernels this library has launched since it was loaded (all handles). */
+uint64_t iq_kernel_launches(void);
+
+/* Apply every queued operation now (asynchronous) / and wait for it. 0 = ok. */
+int iq_statevector_flush(void* sv);
+int iq_statevector_sync(void* sv);
+/* sum_i |a_i|^2 (the reference's unexported StateVector::norm_squared, statevector.cpp:206-213). */
+double iq_statevector_norm(void* sv);
+/* <Z_q> for every qubit q = 0..n-1 in one pass. 0 = ok. */
+int iq_statevector_expval_z_all(void* sv, double* out);
+/* sum_t coeff[t] <P_t> for nterms Pauli strings, each n characters long
+ * (character q acts on qubit q; 'I','X','Y','Z'), exact sums. 0 = ok. */
+int iq_statevector_expval_pauli_sum(void* sv, size_t nterms, const double* coeffs, const char* paulis,
+                                    double* val_real, double* val_imag);
+/* Overwrite the amplitudes from split host arrays (2^n each). 0 = ok. */
+int iq_statevector_set_amplitudes(void* sv, const double* real_in, const double* imag_in);
+/* Device address of the amplitude array (complex128, 2^n), after a flush; the
+ * handle's stream (cudaStream_t) for ordering work against it. */
+void* iq_statevector_device_ptr(void* sv);
+void* iq_statevector_stream(void* sv);
+size_t iq_statevector_num_qubits(void* sv);
+
+/* Tuning / diagnostics for either handle kind.  Keys: "tile_bits", "chunk_bits",
+ * "reg_slots", "max_stages", "budget", "nbuf", "ctas_per_sm", "eager",
+ * "flush_ops", "profile".  0 = ok, -1 = unknown key or bad value. */
+int iq_handle_set_option(void* h, const char* key, double value);
+double iq_handle_get_option(void* h, const char* key);
+/* Counters: out[0] passes, [1] operations applied, [2] algorithmic bytes moved by
+ * passes, [3] kernel launches, [4] flushes, [5] tile-pass launches.  Returns the
+ * number of values written. */
+int iq_handle_stats(void* h, double* out, size_t n);
+/* With option "profile" = 1 every tile pass is bracketed by CUDA events; this
+ * returns up to max per-pass durations in ms (oldest first) and clears them. */
+int iq_handle_profile_read(void* h, double* ms_out, size_t max);
+
+/* Density-matrix additions. */
+int iq_density_matrix_flush(void* dm);
+/* Kraus channel on two qubits: num_kraus 4x4 matrices, q0 = most significant
+ * local bit (the reference declares DensityMatrix::apply_kraus for this,
+ * density_matrix.cpp:165-191, but does not export it). */
+void iq_density_matrix_apply_kraus_2q(void* dm, size_t q0, size_t q1, size_t num_kraus,
+                                      const double* k_real, const double* k_imag);
+/* rho_ii for i = 0..2^n-1. */
+void iq_density_matrix_get_diagonal(void* dm, double* out);
+/* P(qubit target = outcome) = sum of matching diagonal entries. */
+double iq_density_matrix_measure_prob(void* dm, size_t target, int outcome);
+void* iq_density_matrix_device_ptr(void* dm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INVARIANTQ_B200_H */

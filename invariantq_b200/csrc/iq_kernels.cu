@@ -1,0 +1,990 @@
+// iq_kernels.cu -- sm_100a kernels for the state-vector / density-matrix path.
+//
+// Hot kernel: tile_pass_kernel.  One launch = one pass over the complex128
+// array (16 B per amplitude read once, written once).  Per CTA one producer
+// warp moves 2^M-amplitude tiles between HBM and shared memory with TMA tensor
+// copies (cp.async.bulk.tensor, mbarrier completion), through an NBUF-deep ring
+// of tile buffers; the consumer warps apply the pass's register stages (see
+// iq_plan.h) to the resident tile.  This replaces the reference's per-gate
+// OpenMP sweeps (core/src/statevector.cpp:26-152) and its two-pass density-
+// matrix updates (core/src/density_matrix.cpp:18-163): a density matrix is the
+// same array with 2n index bits, U rho U^dagger is U on the row bits and
+// conj(U) on the column bits, and a Kraus channel is the 4x4 superoperator
+// sum_k K_k (x) conj(K_k) on the (row, column) bit pair.
+//
+// Every wait on an mbarrier is bounded; a wait that runs out sets a status word
+// the host reads, and the CTA finishes its loop without further copies.
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "iq_kernels.h"
+
+namespace iqb {
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+__device__ __forceinline__ double2 ld_mat(const double2* m, int i) { return __ldg(m + i); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
+                                             const void* src) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
+      " [%0, {%2, %3, %4, %5, %6}], [%1];" ::"l"(tm),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Bounded wait on an mbarrier phase.  Returns false (and raises the abort flag
+// plus the status word) when the limit runs out, or immediately once aborted.
+__device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                             int* status, int code) {
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*abort_flag) return false;
+  }
+  *abort_flag = 1;
+  atomicCAS(status, 0, code);
+  return false;
+}
+
+// ------------------------------------------------------- register-slot ops
+
+template <int R, int S>
+__device__ __forceinline__ void d1r(double2 (&a)[1 << R], const double2* m) {
+  const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & (1 << S)) continue;
+    const double2 x = a[v], y = a[v | (1 << S)];
+    a[v] = cfma(cmul(u0, x), u1, y);
+    a[v | (1 << S)] = cfma(cmul(u2, x), u3, y);
+  }
+}
+
+template <int R, int S>
+__device__ __forceinline__ void m1r(double2 (&a)[1 << R], const double2* m, int perm, bool unit) {
+  const double2 p0 = ld_mat(m, 0), p1 = ld_mat(m, 1);
+  const bool sw = perm & 1;
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & (1 << S)) continue;
+    double2 x = a[v], y = a[v | (1 << S)];
+    if (sw) { const double2 t = x; x = y; y = t; }
+    if (!unit) { x = cmul(p0, x); y = cmul(p1, y); }
+    a[v] = x;
+    a[v | (1 << S)] = y;
+  }
+}
+
+template <int R, int A, int B>
+__device__ __forceinline__ void d2r(double2 (&a)[1 << R], const double2* m) {
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & ((1 << A) | (1 << B))) continue;
+    const int i0 = v, i1 = v | (1 << A), i2 = v | (1 << B), i3 = v | (1 << A) | (1 << B);
+    const double2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+    double2 o[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double2 acc = cmul(ld_mat(m, 4 * r + 0), x0);
+      acc = cfma(acc, ld_mat(m, 4 * r + 1), x1);
+      acc = cfma(acc, ld_mat(m, 4 * r + 2), x2);
+      acc = cfma(acc, ld_mat(m, 4 * r + 3), x3);
+      o[r] = acc;
+    }
+    a[i0] = o[0];
+    a[i1] = o[1];
+    a[i2] = o[2];
+    a[i3] = o[3];
+  }
+}
+
+__device__ __forceinline__ double2 sel4(int i, double2 x0, double2 x1, double2 x2, double2 x3) {
+  const double2 lo = (i & 1) ? x1 : x0;
+  const double2 hi = (i & 1) ? x3 : x2;
+  return (i & 2) ? hi : lo;
+}
+
+template <int R, int A, int B>
+__device__ __forceinline__ void m2r(double2 (&a)[1 << R], const double2* m, int perm, bool unit) {
+  const int c0 = perm & 3, c1 = (perm >> 2) & 3, c2 = (perm >> 4) & 3, c3 = (perm >> 6) & 3;
+  double2 p0 = make_double2(1.0, 0.0), p1 = p0, p2 = p0, p3 = p0;
+  if (!unit) { p0 = ld_mat(m, 0); p1 = ld_mat(m, 1); p2 = ld_mat(m, 2); p3 = ld_mat(m, 3); }
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & ((1 << A) | (1 << B))) continue;
+    const int i0 = v, i1 = v | (1 << A), i2 = v | (1 << B), i3 = v | (1 << A) | (1 << B);
+    const double2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+    double2 o0 = sel4(c0, x0, x1, x2, x3), o1 = sel4(c1, x0, x1, x2, x3);
+    double2 o2 = sel4(c2, x0, x1, x2, x3), o3 = sel4(c3, x0, x1, x2, x3);
+    if (!unit) { o0 = cmul(p0, o0); o1 = cmul(p1, o1); o2 = cmul(p2, o2); o3 = cmul(p3, o3); }
+    a[i0] = o0;
+    a[i1] = o1;
+    a[i2] = o2;
+    a[i3] = o3;
+  }
+}
+
+// tile offset of register v: OR of the slot bits set in v (v is a compile-time
+// constant after unrolling, so this folds to a few ORs)
+template <int R>
+__device__ __forceinline__ uint32_t voff(int v, const uint32_t (&sb)[R]) {
+  uint32_t o = 0;
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+    if ((v >> i) & 1) o |= sb[i];
+  return o;
+}
+
+// dense 2^K block on slots 0..K-1, written straight to the tile (ends the stage);
+// rows are a runtime loop so only one row of the matrix is live at a time
+template <int R, int K>
+__device__ __forceinline__ void dkr_store(const double2 (&a)[1 << R], const double2* m, double2* tile,
+                                          const uint32_t (&sb)[R], uint32_t base) {
+  constexpr int D = 1 << K;
+#pragma unroll
+  for (int g = 0; g < (1 << R); g += D) {
+    const uint32_t goff = base | voff<R>(g, sb);
+#pragma unroll 1
+    for (int r = 0; r < D; ++r) {
+      double2 acc = cmul(ld_mat(m, r * D), a[g]);
+#pragma unroll
+      for (int c = 1; c < D; ++c) acc = cfma(acc, ld_mat(m, r * D + c), a[g + c]);
+      uint32_t roff = 0;
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((r >> i) & 1) roff |= sb[i];
+      tile[goff | roff] = acc;
+    }
+  }
+}
+
+// lane-bit 1q ops: partner amplitude lives in lane ^ (1 << lb) of the octet
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int d, unsigned mask) {
+  return make_double2(__shfl_xor_sync(mask, v.x, d, 8), __shfl_xor_sync(mask, v.y, d, 8));
+}
+
+template <int R>
+__device__ __forceinline__ void d1l(double2 (&a)[1 << R], const double2* m, int lb, int lane8, unsigned omask) {
+  const int my = (lane8 >> lb) & 1;
+  const double2 cs = my ? ld_mat(m, 3) : ld_mat(m, 0);
+  const double2 co = my ? ld_mat(m, 2) : ld_mat(m, 1);
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    const double2 p = shfl_xor2(a[v], 1 << lb, omask);
+    a[v] = cfma(cmul(cs, a[v]), co, p);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void m1l(double2 (&a)[1 << R], const double2* m, int lb, int lane8, unsigned omask,
+                                    int perm, bool unit) {
+  const int my = (lane8 >> lb) & 1;
+  const double2 ph = unit ? make_double2(1.0, 0.0) : (my ? ld_mat(m, 1) : ld_mat(m, 0));
+  const bool sw = perm & 1;
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    double2 x = a[v];
+    if (sw) x = shfl_xor2(x, 1 << lb, omask);
+    a[v] = unit ? x : cmul(ph, x);
+  }
+}
+
+// ------------------------------------------------------- runtime dispatch
+
+template <int R, int S = 0>
+__device__ __forceinline__ void disp_d1r(int s, double2 (&a)[1 << R], const double2* m) {
+  if constexpr (S < R) {
+    if (s == S) d1r<R, S>(a, m);
+    else disp_d1r<R, S + 1>(s, a, m);
+  }
+}
+template <int R, int S = 0>
+__device__ __forceinline__ void disp_m1r(int s, double2 (&a)[1 << R], const double2* m, int perm, bool unit) {
+  if constexpr (S < R) {
+    if (s == S) m1r<R, S>(a, m, perm, unit);
+    else disp_m1r<R, S + 1>(s, a, m, perm, unit);
+  }
+}
+template <int R, int A, int B = 0>
+__device__ __forceinline__ void disp_d2r_b(int b, double2 (&a)[1 << R], const double2* m) {
+  if constexpr (B < R) {
+    if constexpr (A != B) {
+      if (b == B) { d2r<R, A, B>(a, m); return; }
+    }
+    disp_d2r_b<R, A, B + 1>(b, a, m);
+  }
+}
+template <int R, int A = 0>
+__device__ __forceinline__ void disp_d2r(int sa, int sb, double2 (&a)[1 << R], const double2* m) {
+  if constexpr (A < R) {
+    if (sa == A) disp_d2r_b<R, A>(sb, a, m);
+    else disp_d2r<R, A + 1>(sa, sb, a, m);
+  }
+}
+template <int R, int A, int B = 0>
+__device__ __forceinline__ void disp_m2r_b(int b, double2 (&a)[1 << R], const double2* m, int perm, bool unit) {
+  if constexpr (B < R) {
+    if constexpr (A != B) {
+      if (b == B) { m2r<R, A, B>(a, m, perm, unit); return; }
+    }
+    disp_m2r_b<R, A, B + 1>(b, a, m, perm, unit);
+  }
+}
+template <int R, int A = 0>
+__device__ __forceinline__ void disp_m2r(int sa, int sb, double2 (&a)[1 << R], const double2* m, int perm,
+                                         bool unit) {
+  if constexpr (A < R) {
+    if (sa == A) disp_m2r_b<R, A>(sb, a, m, perm, unit);
+    else disp_m2r<R, A + 1>(sa, sb, a, m, perm, unit);
+  }
+}
+template <int R, int K = 3>
+__device__ __forceinline__ void disp_dkr(int k, const double2 (&a)[1 << R], const double2* m, double2* tile,
+                                         const uint32_t (&sb)[R], uint32_t base) {
+  if constexpr (K <= R) {
+    if (k == K) dkr_store<R, K>(a, m, tile, sb, base);
+    else disp_dkr<R, K + 1>(k, a, m, tile, sb, base);
+  }
+}
+
+// One stage over the resident tile (consumer threads only).
+template <int R>
+__device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int s, const double2* __restrict__ mats,
+                                          int ctid, int ncons) {
+  constexpr int NV = 1 << R;
+  const StageDesc& sd = P.st[s];
+  const int lane8 = ctid & 7;
+  const unsigned omask = 0xFFu << (ctid & 24);
+  const uint32_t laneoff = ((uint32_t)(lane8 & 1) << sd.lane[0]) | ((uint32_t)((lane8 >> 1) & 1) << sd.lane[1]) |
+                           ((uint32_t)((lane8 >> 2) & 1) << sd.lane[2]);
+  uint32_t sb[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) sb[i] = 1u << sd.S[i];
+  const int nsub = 1 << sd.nt;
+  const int op0 = sd.op0, op1 = sd.op1;
+  for (int u = ctid >> 3; u < nsub; u += ncons >> 3) {
+    uint32_t base = laneoff;
+    for (int i = 0; i < sd.nt; ++i) base |= (uint32_t)((u >> i) & 1) << sd.tb[i];
+    double2 a[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a[v] = tile[base | voff<R>(v, sb)];
+    bool stored = false;
+    for (int o = op0; o < op1; ++o) {
+      const OpDesc od = P.ops[o];
+      const double2* m = mats + od.mat;
+      const bool unit = od.flags & OPF_UNIT_PHASE;
+      switch (od.kind) {
+        case OP_D1R: disp_d1r<R>(od.a, a, m); break;
+        case OP_D1L: d1l<R>(a, m, od.a, lane8, omask); break;
+        case OP_D2R: disp_d2r<R>(od.a, od.b, a, m); break;
+        case OP_M1R: disp_m1r<R>(od.a, a, m, od.perm, unit); break;
+        case OP_M1L: m1l<R>(a, m, od.a, lane8, omask, od.perm, unit); break;
+        case OP_M2R: disp_m2r<R>(od.a, od.b, a, m, od.perm, unit); break;
+        case OP_DKR:
+          disp_dkr<R>(od.k, a, m, tile, sb, base);
+          stored = true;
+          break;
+        default: break;
+      }
+    }
+    if (!stored) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) tile[base | voff<R>(v, sb)] = a[v];
+    }
+  }
+}
+
+constexpr int kMaxBuf = 4;
+
+template <int R>
+struct TileCfg {
+  static constexpr int kCons = (R == 4) ? 256 : 128;
+  static constexpr int kThreads = kCons + 32;
+};
+
+template <int R>
+__global__ void __launch_bounds__(TileCfg<R>::kThreads, 1)
+    tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
+                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf) {
+  constexpr int NCONS = TileCfg<R>::kCons;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
+  __shared__ __align__(8) uint64_t bar_computed[kMaxBuf];
+  __shared__ volatile int abort_flag;
+
+  double2* tiles = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x;
+  const uint32_t tile_elems = 1u << P.M;
+  if (tid == 0) {
+    for (int b = 0; b < nbuf; ++b) {
+      mbar_init(&bar_loaded[b], 1);
+      mbar_init(&bar_computed[b], 1);
+    }
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  const uint64_t ntiles = P.ntiles;
+  const uint64_t first = blockIdx.x;
+  const uint64_t cnt = (first < ntiles) ? (ntiles - 1 - first) / gridDim.x + 1 : 0;
+
+  if (tid >= NCONS) {
+    // ---------------- producer warp: lane 0 drives TMA
+    if (tid != NCONS) return;
+    const int nbox = P.nbox;
+    const int nissue_bits = P.nH - nbox;
+    const int nissue = 1 << nissue_bits;
+    const uint32_t box_elems = 1u << (P.c + nbox);
+    const uint32_t bytes = tile_elems * 16u;
+    auto do_store = [&](uint64_t i) {
+      const int b = (int)(i % nbuf);
+      const uint64_t base = tile_base(first + i * gridDim.x, P);
+      double2* buf = tiles + (size_t)b * tile_elems;
+      for (int j = 0; j < nissue; ++j) {
+        int c1, c2, c3, c4;
+        chunk_coords(base | issue_offset(j, P), P, c1, c2, c3, c4);
+        tma_store_5d(&tm, 0, c1, c2, c3, c4, buf + (size_t)j * box_elems);
+      }
+      bulk_commit();
+    };
+    for (uint64_t i = 0; i < cnt; ++i) {
+      const int b = (int)(i % nbuf);
+      if (i >= (uint64_t)nbuf) {
+        const uint64_t prev = i - nbuf;
+        const bool ok = bounded_wait(&bar_computed[b], (uint32_t)((prev / nbuf) & 1), &abort_flag, status,
+                                     DEV_WAIT_COMPUTED);
+        if (ok && !abort_flag) do_store(prev);
+        bulk_wait_read_all();
+      }
+      if (abort_flag) {
+        mbar_arrive(&bar_loaded[b]);   // let the consumers' bounded wait see the phase
+        continue;
+      }
+      const uint64_t base = tile_base(first + i * gridDim.x, P);
+      double2* buf = tiles + (size_t)b * tile_elems;
+      mbar_arrive_expect_tx(&bar_loaded[b], bytes);
+      for (int j = 0; j < nissue; ++j) {
+        int c1, c2, c3, c4;
+        chunk_coords(base | issue_offset(j, P), P, c1, c2, c3, c4);
+        tma_load_5d(buf + (size_t)j * box_elems, &tm, 0, c1, c2, c3, c4, &bar_loaded[b]);
+      }
+    }
+    const uint64_t tail0 = cnt > (uint64_t)nbuf ? cnt - nbuf : 0;
+    for (uint64_t i = tail0; i < cnt; ++i) {
+      const int b = (int)(i % nbuf);
+      const bool ok = bounded_wait(&bar_computed[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status,
+                                   DEV_WAIT_COMPUTED);
+      if (ok && !abort_flag) do_store(i);
+    }
+    bulk_wait_all();
+    return;
+  }
+
+  // ---------------- consumers
+  for (uint64_t i = 0; i < cnt; ++i) {
+    const int b = (int)(i % nbuf);
+    double2* buf = tiles + (size_t)b * tile_elems;
+    const bool ok = bounded_wait(&bar_loaded[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status,
+                                 DEV_WAIT_LOADED);
+    const bool work = ok && !abort_flag;
+    for (int s = 0; s < P.nstages; ++s) {
+      if (work) run_stage<R>(buf, P, s, mats, tid, NCONS);
+      consumer_sync(NCONS);
+    }
+    fence_proxy_async_smem();
+    consumer_sync(NCONS);
+    if (tid == 0) mbar_arrive(&bar_computed[b]);
+  }
+}
+
+size_t tile_pass_smem_bytes(int M, int nbuf) { return (size_t)nbuf * (16u << M) + 1024; }
+
+cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
+                             const TileLaunch& tl, int num_sms, cudaStream_t st) {
+  const int nbuf = tl.nbuf < 1 ? 1 : (tl.nbuf > kMaxBuf ? kMaxBuf : tl.nbuf);
+  const size_t smem = tile_pass_smem_bytes(d.M, nbuf);
+  uint64_t grid = (uint64_t)num_sms * (uint64_t)(tl.ctas_per_sm < 1 ? 1 : tl.ctas_per_sm);
+  if (grid > d.ntiles) grid = d.ntiles;
+  cudaError_t e;
+  if (d.R == 4) {
+    e = cudaFuncSetAttribute(tile_pass_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tile_pass_kernel<4><<<(unsigned)grid, TileCfg<4>::kThreads, smem, st>>>(tm, d, mats, dev_status, nbuf);
+  } else {
+    e = cudaFuncSetAttribute(tile_pass_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    tile_pass_kernel<5><<<(unsigned)grid, TileCfg<5>::kThreads, smem, st>>>(tm, d, mats, dev_status, nbuf);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ tensor maps
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d, char* err, size_t errlen) {
+  auto fn = encode_fn();
+  if (!fn) {
+    snprintf(err, errlen, "cuTensorMapEncodeTiled unavailable from the driver");
+    return -1;
+  }
+  uint64_t g[5], st[4];
+  uint32_t b[5];
+  pass_tmap_layout(d, nbits, g, st, b);
+  cuuint64_t gd[5], gs[4];
+  cuuint32_t box[5], es[5] = {1, 1, 1, 1, 1};
+  for (int i = 0; i < 5; ++i) { gd[i] = g[i]; box[i] = b[i]; }
+  for (int i = 0; i < 4; ++i) gs[i] = st[i];
+  CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, state, gd, gs, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    snprintf(err, errlen, "cuTensorMapEncodeTiled failed (%d) for nbits=%d c=%d nbox=%d", (int)r, nbits, (int)d.c,
+             (int)d.nbox);
+    return -1;
+  }
+  return 0;
+}
+
+// ------------------------------------------------------- simple path
+
+struct SimpleArgs {
+  int k;
+  int q[kMaxK];
+  int qs[kMaxK];   // sorted ascending
+  uint32_t mat;
+};
+
+template <int K>
+__global__ void simple_op_kernel(double2* __restrict__ s, int nbits, SimpleArgs a, const double2* __restrict__ mats) {
+  constexpr int D = 1 << K;
+  const uint64_t groups = 1ULL << (nbits - K);
+  const double2* m = mats + a.mat;
+  uint64_t qb[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) qb[i] = 1ULL << a.q[i];
+  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < groups;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t base = g;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      const int h = a.qs[i];
+      base = ((base >> h) << (h + 1)) | (base & ((1ULL << h) - 1));
+    }
+    double2 x[D];
+#pragma unroll
+    for (int v = 0; v < D; ++v) {
+      uint64_t id = base;
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((v >> i) & 1) id |= qb[i];
+      x[v] = s[id];
+    }
+#pragma unroll 1
+    for (int r = 0; r < D; ++r) {
+      double2 acc = cmul(ld_mat(m, r * D), x[0]);
+#pragma unroll
+      for (int c = 1; c < D; ++c) acc = cfma(acc, ld_mat(m, r * D + c), x[c]);
+      uint64_t id = base;
+#pragma unroll
+      for (int i = 0; i < K; ++i)
+        if ((r >> i) & 1) id |= qb[i];
+      s[id] = acc;
+    }
+  }
+}
+
+static unsigned grid_for(uint64_t work, int threads) {
+  uint64_t g = (work + threads - 1) / threads;
+  const uint64_t cap = 148ull * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+cudaError_t launch_simple_op(double2* s, int nbits, const SimpleOp& op, const double2* mats, cudaStream_t st) {
+  SimpleArgs a;
+  a.k = op.k;
+  a.mat = op.mat;
+  for (int i = 0; i < op.k; ++i) a.q[i] = a.qs[i] = op.q[i];
+  for (int i = 0; i < op.k; ++i)
+    for (int j = i + 1; j < op.k; ++j)
+      if (a.qs[j] < a.qs[i]) { int t = a.qs[i]; a.qs[i] = a.qs[j]; a.qs[j] = t; }
+  const uint64_t groups = 1ULL << (nbits - op.k);
+  const int th = 128;
+  const unsigned g = grid_for(groups, th);
+  switch (op.k) {
+    case 1: simple_op_kernel<1><<<g, th, 0, st>>>(s, nbits, a, mats); break;
+    case 2: simple_op_kernel<2><<<g, th, 0, st>>>(s, nbits, a, mats); break;
+    case 3: simple_op_kernel<3><<<g, th, 0, st>>>(s, nbits, a, mats); break;
+    case 4: simple_op_kernel<4><<<g, th, 0, st>>>(s, nbits, a, mats); break;
+    case 5: simple_op_kernel<5><<<g, th, 0, st>>>(s, nbits, a, mats); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ reductions
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block-wide sum; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+    t = warp_sum(t);
+  }
+  return t;
+}
+
+__global__ void final_sum_kernel(const double* __restrict__ p, int n, double* __restrict__ out) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) *out = v;
+}
+
+__global__ void sumsq_masked_kernel(const double2* __restrict__ s, uint64_t dim, uint64_t mask, uint64_t val,
+                                    double* __restrict__ partials) {
+  double acc = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+    if ((i & mask) == val) {
+      const double2 a = s[i];
+      acc += a.x * a.x + a.y * a.y;
+    }
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+cudaError_t launch_sumsq_masked(const double2* s, uint64_t dim, uint64_t mask, uint64_t val, double* partials,
+                                double* out, cudaStream_t st) {
+  sumsq_masked_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(s, dim, mask, val, partials);
+  final_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, out);
+  return cudaGetLastError();
+}
+
+__global__ void diag_sum_kernel(const double2* __restrict__ rho, uint64_t dim, uint64_t mask, uint64_t val,
+                                double* __restrict__ partials) {
+  double acc = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x)
+    if ((i & mask) == val) acc += rho[i * (dim + 1)].x;
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+cudaError_t launch_diag_sum(const double2* rho, uint64_t dim, uint64_t mask, uint64_t val, double* partials,
+                            double* out, cudaStream_t st) {
+  diag_sum_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(rho, dim, mask, val, partials);
+  final_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, out);
+  return cudaGetLastError();
+}
+
+__global__ void diag_entropy_kernel(const double2* __restrict__ rho, uint64_t dim, double* __restrict__ partials) {
+  double acc = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+    double p = rho[i * (dim + 1)].x;
+    if (p < 0.0) p = 0.0;
+    if (p > 1e-14) acc -= p * log2(p);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+cudaError_t launch_diag_entropy(const double2* rho, uint64_t dim, double* partials, double* out, cudaStream_t st) {
+  diag_entropy_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(rho, dim, partials);
+  final_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, out);
+  return cudaGetLastError();
+}
+
+__global__ void pauli_sum_kernel(const double2* __restrict__ s, uint64_t dim, uint64_t xmask, uint64_t zmask,
+                                 double thresh, double2* __restrict__ partials) {
+  double re = 0.0, im = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 a = s[i];
+    if (a.x * a.x + a.y * a.y < thresh) continue;
+    const double2 b = s[i ^ xmask];
+    // conj(b) * a
+    double pr = b.x * a.x + b.y * a.y;
+    double pi = b.x * a.y - b.y * a.x;
+    if (__popcll(i & zmask) & 1) { pr = -pr; pi = -pi; }
+    re += pr;
+    im += pi;
+  }
+  re = block_sum(re);
+  im = block_sum(im);
+  if (threadIdx.x == 0) partials[blockIdx.x] = make_double2(re, im);
+}
+
+__global__ void final_csum_kernel(const double2* __restrict__ p, int n, double2* __restrict__ out) {
+  double re = 0.0, im = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    re += p[i].x;
+    im += p[i].y;
+  }
+  re = block_sum(re);
+  im = block_sum(im);
+  if (threadIdx.x == 0) *out = make_double2(re, im);
+}
+
+cudaError_t launch_pauli_sum(const double2* s, uint64_t dim, uint64_t xmask, uint64_t zmask, double thresh,
+                             double2* partials, double2* out, cudaStream_t st) {
+  pauli_sum_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(s, dim, xmask, zmask, thresh, partials);
+  final_csum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, out);
+  return cudaGetLastError();
+}
+
+// Per-bit occupation sums.  Thread layout: blocks sweep super-chunks of
+// 256 * 8 consecutive amplitudes; within one, element j*256 + tid has bits 0..7
+// = tid, bits 8..10 = j, higher bits from the super-chunk index.
+constexpr int kZThreads = 256;
+constexpr int kZJ = 8;
+constexpr int kZMaxBits = 40;
+
+size_t zsums_partials_doubles(int nbits) { return (size_t)kRedBlocks * (nbits + 1); }
+
+__global__ void zsums_kernel(const double2* __restrict__ s, int nbits, double* __restrict__ partials) {
+  const uint64_t dim = 1ULL << nbits;
+  const uint64_t chunk = (uint64_t)kZThreads * kZJ;
+  double tot = 0.0, sj[3] = {0.0, 0.0, 0.0};
+  double hi[kZMaxBits - 11];
+#pragma unroll
+  for (int b = 0; b < kZMaxBits - 11; ++b) hi[b] = 0.0;
+  const int tid = threadIdx.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * chunk; base < dim; base += (uint64_t)gridDim.x * chunk) {
+    double ct = 0.0;
+#pragma unroll
+    for (int j = 0; j < kZJ; ++j) {
+      const uint64_t i = base + (uint64_t)j * kZThreads + tid;
+      if (i < dim) {
+        const double2 a = s[i];
+        const double p = a.x * a.x + a.y * a.y;
+        ct += p;
+        if (j & 1) sj[0] += p;
+        if (j & 2) sj[1] += p;
+        if (j & 4) sj[2] += p;
+      }
+    }
+    tot += ct;
+#pragma unroll
+    for (int b = 11; b < kZMaxBits; ++b)
+      if (b < nbits && ((base >> b) & 1)) hi[b - 11] += ct;
+  }
+  // bit b < 8: whole thread total if tid bit set; 8..10: sj; >= 11: hi
+#pragma unroll
+  for (int b = 0; b <= kZMaxBits; ++b) {
+    if (b > nbits) break;
+    double v;
+    if (b == 0) v = tot;
+    else {
+      const int bit = b - 1;
+      if (bit < 8) v = ((tid >> bit) & 1) ? tot : 0.0;
+      else if (bit < 11) v = sj[bit - 8];
+      else v = hi[bit - 11];
+    }
+    v = block_sum(v);
+    if (threadIdx.x == 0) partials[(size_t)b * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+__global__ void zsums_final_kernel(const double* __restrict__ partials, int nblocks, int nvals, double* __restrict__ out) {
+  const int b = blockIdx.x;
+  if (b >= nvals) return;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) v += partials[(size_t)b * nblocks + i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) out[b] = v;
+}
+
+cudaError_t launch_zsums(const double2* s, int nbits, double* partials, double* out, cudaStream_t st) {
+  if (nbits > kZMaxBits) return cudaErrorInvalidValue;
+  zsums_kernel<<<kRedBlocks, kZThreads, 0, st>>>(s, nbits, partials);
+  zsums_final_kernel<<<nbits + 1, 256, 0, st>>>(partials, kRedBlocks, nbits + 1, out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ elementwise
+
+__global__ void collapse_kernel(double2* __restrict__ s, uint64_t dim, uint64_t mask, uint64_t val, double f) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x) {
+    if ((i & mask) == val) {
+      double2 a = s[i];
+      a.x *= f;
+      a.y *= f;
+      s[i] = a;
+    } else {
+      s[i] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+cudaError_t launch_collapse(double2* s, uint64_t dim, uint64_t mask, uint64_t val, double factor, cudaStream_t st) {
+  collapse_kernel<<<grid_for(dim, 256), 256, 0, st>>>(s, dim, mask, val, factor);
+  return cudaGetLastError();
+}
+
+__global__ void dm_collapse_kernel(double2* __restrict__ rho, int n, uint64_t mask, uint64_t val, double f) {
+  const uint64_t dim = 1ULL << n, tot = dim * dim;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < tot; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = i >> n, c = i & (dim - 1);
+    if ((r & mask) == val && (c & mask) == val) {
+      double2 a = rho[i];
+      a.x *= f;
+      a.y *= f;
+      rho[i] = a;
+    } else {
+      rho[i] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+cudaError_t launch_dm_collapse(double2* rho, int n, uint64_t mask, uint64_t val, double factor, cudaStream_t st) {
+  const uint64_t tot = 1ULL << (2 * n);
+  dm_collapse_kernel<<<grid_for(tot, 256), 256, 0, st>>>(rho, n, mask, val, factor);
+  return cudaGetLastError();
+}
+
+__global__ void set_basis_kernel(double2* __restrict__ s, uint64_t dim) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim; i += (uint64_t)gridDim.x * blockDim.x)
+    s[i] = make_double2(i == 0 ? 1.0 : 0.0, 0.0);
+}
+
+cudaError_t launch_set_basis(double2* s, uint64_t dim, cudaStream_t st) {
+  set_basis_kernel<<<grid_for(dim, 256), 256, 0, st>>>(s, dim);
+  return cudaGetLastError();
+}
+
+__global__ void split_kernel(const double2* __restrict__ s, uint64_t n, double* __restrict__ re, double* __restrict__ im) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 a = s[i];
+    re[i] = a.x;
+    im[i] = a.y;
+  }
+}
+
+cudaError_t launch_split(const double2* s, uint64_t count, double* re, double* im, cudaStream_t st) {
+  split_kernel<<<grid_for(count, 256), 256, 0, st>>>(s, count, re, im);
+  return cudaGetLastError();
+}
+
+__global__ void probs_kernel(const double2* __restrict__ s, uint64_t n, double* __restrict__ p) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 a = s[i];
+    p[i] = a.x * a.x + a.y * a.y;
+  }
+}
+
+cudaError_t launch_probs(const double2* s, uint64_t count, double* p, cudaStream_t st) {
+  probs_kernel<<<grid_for(count, 256), 256, 0, st>>>(s, count, p);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ sampling
+
+__global__ void block_sums_kernel(const double2* __restrict__ s, uint64_t nblk, int bbits, double* __restrict__ out) {
+  // one warp per block of 2^bbits amplitudes, summed in index order per lane then across lanes
+  const int lane = threadIdx.x & 31;
+  const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t len = 1ULL << bbits;
+  for (uint64_t b = w; b < nblk; b += nw) {
+    double acc = 0.0;
+    for (uint64_t i = lane; i < len; i += 32) {
+      const double2 a = s[b * len + i];
+      acc += a.x * a.x + a.y * a.y;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out[b] = acc;
+  }
+}
+
+cudaError_t launch_block_sums(const double2* s, uint64_t dim, int bbits, double* out, cudaStream_t st) {
+  const uint64_t nblk = dim >> bbits;
+  block_sums_kernel<<<grid_for(nblk * 32, 256), 256, 0, st>>>(s, nblk, bbits, out);
+  return cudaGetLastError();
+}
+
+__global__ void block_search_kernel(const double2* __restrict__ s, int bbits, const uint64_t* __restrict__ blk,
+                                    const double* __restrict__ base, const double* __restrict__ target,
+                                    uint64_t* __restrict__ out, int shots) {
+  // one warp per shot: sequential 32-wide windows, inclusive warp scan
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= shots) return;
+  const uint64_t len = 1ULL << bbits;
+  const uint64_t b0 = blk[w] * len;
+  double run = base[w];
+  const double r = target[w];
+  uint64_t found = b0 + len - 1;
+  for (uint64_t off = 0; off < len; off += 32) {
+    const double2 a = s[b0 + off + lane];
+    double v = a.x * a.x + a.y * a.y;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const double t = __shfl_up_sync(0xffffffffu, v, d);
+      if (lane >= d) v += t;
+    }
+    const double cum = run + v;
+    const unsigned hit = __ballot_sync(0xffffffffu, cum >= r);
+    if (hit) {
+      found = b0 + off + (__ffs(hit) - 1);
+      break;
+    }
+    run += __shfl_sync(0xffffffffu, v, 31);
+  }
+  if (lane == 0) out[w] = found;
+}
+
+cudaError_t launch_block_search(const double2* s, int bbits, const uint64_t* blk, const double* base,
+                                const double* target, uint64_t* out, int shots, cudaStream_t st) {
+  if (shots <= 0) return cudaSuccess;
+  const int th = 256;
+  const int blocks = (shots * 32 + th - 1) / th;
+  block_search_kernel<<<blocks, th, 0, st>>>(s, bbits, blk, base, target, out, shots);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------- partial trace (entropy)
+
+struct KeepArgs {
+  int k;
+  int keep[12];
+  int nt;
+  int traced[40];
+};
+
+__global__ void partial_trace_kernel(const double2* __restrict__ s, KeepArgs a, double2* __restrict__ out) {
+  // one block per (r, c) with r <= c; threads sweep the environment
+  const uint64_t kd = 1ULL << a.k;
+  const uint64_t pair = blockIdx.x;
+  // decode upper-triangle pair index
+  uint64_t r = 0, rem = pair;
+  while (rem >= kd - r) { rem -= kd - r; ++r; }
+  const uint64_t c = r + rem;
+  uint64_t ir = 0, ic = 0;
+  for (int b = 0; b < a.k; ++b) {
+    if ((r >> b) & 1) ir |= 1ULL << a.keep[b];
+    if ((c >> b) & 1) ic |= 1ULL << a.keep[b];
+  }
+  const uint64_t td = 1ULL << a.nt;
+  double re = 0.0, im = 0.0;
+  for (uint64_t env = threadIdx.x; env < td; env += blockDim.x) {
+    uint64_t e = 0;
+    for (int b = 0; b < a.nt; ++b)
+      if ((env >> b) & 1) e |= 1ULL << a.traced[b];
+    const double2 x = s[ir | e], y = s[ic | e];
+    // x * conj(y)
+    re += x.x * y.x + x.y * y.y;
+    im += x.y * y.x - x.x * y.y;
+  }
+  re = block_sum(re);
+  im = block_sum(im);
+  if (threadIdx.x == 0) {
+    out[r * kd + c] = make_double2(re, im);
+    out[c * kd + r] = make_double2(re, -im);
+  }
+}
+
+cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, int k, double2* out, cudaStream_t st) {
+  if (k < 1 || k > 12) return cudaErrorInvalidValue;
+  KeepArgs a;
+  a.k = k;
+  for (int i = 0; i < k; ++i) a.keep[i] = keep[i];
+  a.nt = 0;
+  for (int q = 0; q < nbits; ++q) {
+    bool in = false;
+    for (int i = 0; i < k; ++i) in |= keep[i] == q;
+    if (!in) a.traced[a.nt++] = q;
+  }
+  const uint64_t kd = 1ULL << k;
+  const uint64_t npairs = kd * (kd + 1) / 2;
+  partial_trace_kernel<<<(unsigned)npairs, 256, 0, st>>>(s, a, out);
+  return cudaGetLastError();
+}
+
+}  // namespace iqb

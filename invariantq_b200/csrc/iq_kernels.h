@@ -1,0 +1,77 @@
+// iq_kernels.h -- launchers for the sm_100a kernels in iq_kernels.cu.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "iq_plan.h"
+
+namespace iqb {
+
+// Error codes a kernel can raise in the per-handle device status word.
+enum DevErr : int {
+  DEV_OK = 0,
+  DEV_WAIT_LOADED = 1,     // a tile load did not complete in the wait limit
+  DEV_WAIT_COMPUTED = 2,   // the producer waited too long for the consumers
+};
+
+struct TileLaunch {
+  int nbuf;                // shared-memory tile buffers per CTA (pipeline depth)
+  int ctas_per_sm;         // resident CTAs per SM the grid is sized for
+};
+
+// Encode the pass tensor map for `state` (2^nbits complex128).
+int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d, char* err, size_t errlen);
+
+// Launch one tile pass.  `mats` is the device copy of the flush's matrix pool.
+cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
+                             const TileLaunch& tl, int num_sms, cudaStream_t st);
+size_t tile_pass_smem_bytes(int M, int nbuf);
+
+// Simple path: one operation straight in global memory (k = 1..5, LSB-first bits).
+struct SimpleOp {
+  int k;
+  int q[kMaxK];
+  uint32_t mat;            // dense 2^k x 2^k row-major matrix in `mats`
+};
+cudaError_t launch_simple_op(double2* s, int nbits, const SimpleOp& op, const double2* mats, cudaStream_t st);
+
+// ---- reductions (deterministic: fixed grid, partials summed in order) ----
+constexpr int kRedBlocks = 592;    // 4 * 148 SMs
+constexpr int kRedThreads = 256;
+// sum |s_i|^2 over i with (i & mask) == val
+cudaError_t launch_sumsq_masked(const double2* s, uint64_t dim, uint64_t mask, uint64_t val, double* partials,
+                                double* out, cudaStream_t st);
+// sum Re rho_ii (rho is dim x dim row-major) over i with (i & mask) == val
+cudaError_t launch_diag_sum(const double2* rho, uint64_t dim, uint64_t mask, uint64_t val, double* partials,
+                            double* out, cudaStream_t st);
+// sum over the diagonal of -p log2 p, p = max(0, Re rho_ii), p > 1e-14
+cudaError_t launch_diag_entropy(const double2* rho, uint64_t dim, double* partials, double* out, cudaStream_t st);
+// <psi| P |psi> core sum: sum_i [skip if |a_i|^2 < thresh] (-1)^popc(i & zmask) conj(a_{i^xmask}) a_i
+cudaError_t launch_pauli_sum(const double2* s, uint64_t dim, uint64_t xmask, uint64_t zmask, double thresh,
+                             double2* partials, double2* out, cudaStream_t st);
+// out[0] = sum |a|^2, out[1 + b] = sum over i with bit b set of |a_i|^2, b < nbits
+cudaError_t launch_zsums(const double2* s, int nbits, double* partials, double* out, cudaStream_t st);
+size_t zsums_partials_doubles(int nbits);
+
+// ---- elementwise ----
+cudaError_t launch_collapse(double2* s, uint64_t dim, uint64_t mask, uint64_t val, double factor, cudaStream_t st);
+// rho[r][c] *= factor if bits(r) and bits(c) at mask both equal val, else 0
+cudaError_t launch_dm_collapse(double2* rho, int n, uint64_t mask, uint64_t val, double factor, cudaStream_t st);
+cudaError_t launch_set_basis(double2* s, uint64_t dim, cudaStream_t st);   // s = e_0
+cudaError_t launch_split(const double2* s, uint64_t count, double* re, double* im, cudaStream_t st);
+cudaError_t launch_probs(const double2* s, uint64_t count, double* p, cudaStream_t st);
+
+// ---- sampling ----
+// block sums of |a|^2 over blocks of 2^bbits amplitudes
+cudaError_t launch_block_sums(const double2* s, uint64_t dim, int bbits, double* out, cudaStream_t st);
+// for each shot: within block blk[k], the first index whose running sum (starting at base[k])
+// reaches target[k]; falls back to the block's last index
+cudaError_t launch_block_search(const double2* s, int bbits, const uint64_t* blk, const double* base,
+                                const double* target, uint64_t* out, int shots, cudaStream_t st);
+
+// ---- reduced density matrix for entropy ----
+// rho_A[r][c] = sum_env a[idx(r,env)] conj(a[idx(c,env)]), keep[] LSB-first (k <= 12)
+cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, int k, double2* out, cudaStream_t st);
+
+}  // namespace iqb

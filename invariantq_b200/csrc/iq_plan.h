@@ -1,0 +1,197 @@
+// iq_plan.h -- the contract between the host gate scheduler (iq_sched.cpp) and
+// the device tile-pass kernel (iq_kernels.cu).
+//
+// A *pass* streams the whole amplitude array through shared memory once (one
+// read + one write of 16 B per amplitude).  The array is cut into tiles of 2^M
+// amplitudes: a tile holds every combination of M "tile-local" index bits for
+// one fixed value of all other bits.  Tile-local bit j < c is physical bit j
+// (a contiguous chunk of 2^c amplitudes); tile-local bit c + i is physical bit
+// H[i] (H ascending).  Inside the tile the pass runs a list of *stages*; in a
+// stage each thread holds 2^R amplitudes in registers (the R "register slots"
+// S[0..R-1] are tile-local bits), eight consecutive lanes (an octet) span three
+// more "lane" bits, and the remaining "thread" bits enumerate the octets.  A
+// stage applies its operations to the registers (lane-bit operations use warp
+// shuffles inside the octet) and writes the registers back.
+//
+// All operation matrices use one convention: for an operation on qubit list
+// q[0..k-1], bit i of the 2^k local row/column index is qubit q[i] (LSB-first).
+// The C ABI's 2-qubit calls (q0 = most significant) are converted to this form
+// before they reach the scheduler.
+#pragma once
+#include <stdint.h>
+#include <stddef.h>
+
+#if defined(__CUDACC__)
+#define IQ_HD __host__ __device__ __forceinline__
+#else
+#define IQ_HD inline
+#endif
+
+namespace iqb {
+
+constexpr int kMaxTileBits = 13;   // 2^13 amplitudes * 16 B = 128 KiB of shared memory
+constexpr int kLaneBits = 3;       // octet = 8 lanes
+constexpr int kMaxStages = 24;
+constexpr int kMaxPassOps = 160;
+constexpr int kMaxK = 5;           // widest dense block the kernels apply
+
+enum OpKind : uint8_t {
+  OP_NONE = 0,
+  OP_D1R = 1,   // dense 2x2, register slot a
+  OP_D1L = 2,   // dense 2x2, lane bit a
+  OP_D2R = 3,   // dense 4x4, register slots a (matrix bit 0) and b (matrix bit 1)
+  OP_DKR = 4,   // dense 2^k x 2^k, register slots 0..k-1 (matrix bit i = slot i); ends its stage
+  OP_M1R = 5,   // monomial 2x2 (permutation + phases), register slot a
+  OP_M1L = 6,   // monomial 2x2, lane bit a
+  OP_M2R = 7,   // monomial 4x4, register slots a (bit 0) and b (bit 1)
+};
+
+// flags
+constexpr uint8_t OPF_UNIT_PHASE = 1;  // monomial whose phases are all exactly 1
+
+struct OpDesc {          // 16 bytes
+  uint8_t kind;
+  uint8_t a, b, k;
+  uint8_t perm;          // monomial: row r reads column (perm >> (2r)) & 3 (1q: bit 0 = swap)
+  uint8_t flags;
+  uint8_t pad0, pad1;
+  uint32_t mat;          // offset (complex elements) into the flush's matrix buffer
+  uint32_t pad2;
+};
+
+struct StageDesc {       // 28 bytes
+  uint8_t S[kMaxK];      // register slot -> tile-local bit
+  uint8_t lane[kLaneBits];
+  uint8_t nt;            // number of thread bits
+  uint8_t tb[kMaxTileBits];
+  uint16_t op0, op1;     // operation range [op0, op1)
+  uint16_t pad;
+};
+
+struct PassDesc {
+  uint8_t M, c, R, nstages;
+  uint8_t nH, nbox, pad0, pad1;
+  uint8_t H[kMaxTileBits + 3];   // physical bit of tile-local bit c + i (ascending)
+  uint64_t ntiles;
+  uint32_t nops, pad2;
+  StageDesc st[kMaxStages];
+  OpDesc ops[kMaxPassOps];
+};
+
+// One queued gate / channel as the scheduler sees it.
+struct SchedOp {
+  uint8_t k;             // 1..5
+  uint8_t q[kMaxK];      // index bits, LSB-first matrix convention
+  uint8_t mono;          // 1 = monomial matrix (perm + phases)
+  uint8_t perm;          // monomial permutation (see OpDesc)
+  uint8_t unit;          // monomial with unit phases
+  uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
+};
+
+struct SchedParams {
+  int nbits;             // index bits of the array (SV: n, DM: 2n)
+  int M;                 // tile bits
+  int c;                 // contiguous chunk bits (>= 3)
+  int R;                 // register slots per thread (4 or 5)
+  int max_stages;        // stages per pass (each costs one shared-memory round trip)
+  double budget;         // max arithmetic cost per pass (real FMAs per amplitude)
+};
+
+// A planned pass.  desc.ops[].mat are offsets into the caller's op matrix pool
+// (SchedOp::mat), so the pool uploaded once per flush serves every pass.
+struct PassPlan {
+  PassDesc desc;
+  int nsrc;              // number of scheduled ops
+  double cost;           // planned arithmetic cost per amplitude
+};
+
+// Cost (real multiply-adds per amplitude) of applying an operation in a pass.
+double op_cost(const SchedOp& op);
+
+// ---- tile addressing, shared by the kernel and the CPU emulator in tests/ ----
+
+// Amplitude index of element 0 of tile t: t's bits are spread over the
+// non-tile bit positions (all bits except [0, c) and H).
+IQ_HD uint64_t tile_base(uint64_t t, const PassDesc& P) {
+  uint64_t x = t << P.c;
+  for (int i = 0; i < P.nH; ++i) {
+    const int h = P.H[i];
+    x = ((x >> h) << (h + 1)) | (x & ((1ULL << h) - 1));
+  }
+  return x;
+}
+
+// Offset of TMA issue j inside a tile: issue j covers the tile bits H[nbox..].
+IQ_HD uint64_t issue_offset(int j, const PassDesc& P) {
+  uint64_t off = 0;
+  const int nb = P.nH - P.nbox;
+  for (int i = 0; i < nb; ++i)
+    if ((j >> i) & 1) off |= 1ULL << P.H[P.nbox + i];
+  return off;
+}
+
+// 5-D view of the array used by the pass tensor map (dimension 0 innermost,
+// counted in doubles; strides in bytes for dimensions 1..4).  The bits of the
+// amplitude index are cut at the first two tile bits H[0], H[1]:
+//   dim0 = the 2^c-amplitude chunk, dim1 = bits [c, H0), dim2 = bit H0,
+//   dim3 = bits (H0, H1), dim4 = bits [H1, nbits).
+// The box takes the whole chunk and both values of H0 and H1, so one copy
+// moves 2^(c + nbox) amplitudes; the other tile bits are enumerated by issues.
+IQ_HD void pass_tmap_layout(const PassDesc& d, int nbits, uint64_t gd[5], uint64_t gs[4], uint32_t box[5]) {
+  const int c = d.c;
+  const uint64_t E = 16;
+  const uint64_t inner = 2ull << c;
+  const uint64_t top = (1ull << nbits) * E;
+  if (d.nbox == 2) {
+    const int h0 = d.H[0], h1 = d.H[1];
+    gd[0] = inner; gd[1] = 1ull << (h0 - c); gd[2] = 2; gd[3] = 1ull << (h1 - h0 - 1); gd[4] = 1ull << (nbits - h1);
+    gs[0] = (1ull << c) * E; gs[1] = (1ull << h0) * E; gs[2] = (1ull << (h0 + 1)) * E; gs[3] = (1ull << h1) * E;
+    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 2; box[3] = 1; box[4] = 2;
+  } else if (d.nbox == 1) {
+    const int h0 = d.H[0];
+    gd[0] = inner; gd[1] = 1ull << (h0 - c); gd[2] = 1ull << (nbits - h0); gd[3] = 1; gd[4] = 1;
+    gs[0] = (1ull << c) * E; gs[1] = (1ull << h0) * E; gs[2] = top; gs[3] = top;
+    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 2; box[3] = 1; box[4] = 1;
+  } else {
+    gd[0] = inner; gd[1] = 1ull << (nbits - c); gd[2] = 1; gd[3] = 1; gd[4] = 1;
+    gs[0] = (1ull << c) * E; gs[1] = top; gs[2] = top; gs[3] = top;
+    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 1; box[3] = 1; box[4] = 1;
+  }
+}
+
+// Tensor-map coordinates (dims 1..4) of the copy whose first amplitude is A.
+IQ_HD void chunk_coords(uint64_t A, const PassDesc& P, int& c1, int& c2, int& c3, int& c4) {
+  const int c = P.c;
+  if (P.nbox == 2) {
+    const int h0 = P.H[0], h1 = P.H[1];
+    c1 = (int)((A >> c) & ((1ULL << (h0 - c)) - 1));
+    c2 = 0;
+    c3 = (int)((A >> (h0 + 1)) & ((1ULL << (h1 - h0 - 1)) - 1));
+    c4 = (int)(A >> h1);
+  } else if (P.nbox == 1) {
+    const int h0 = P.H[0];
+    c1 = (int)((A >> c) & ((1ULL << (h0 - c)) - 1));
+    c2 = (int)(A >> h0);
+    c3 = 0;
+    c4 = 0;
+  } else {
+    c1 = (int)(A >> c);
+    c2 = c3 = c4 = 0;
+  }
+}
+
+// Plan passes for ops[0..nops): returns the number of passes written to out
+// (growing the vector), or -1 with a message in err on failure.
+}  // namespace iqb
+
+#ifdef __cplusplus
+#include <string>
+#include <vector>
+namespace iqb {
+int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vector<PassPlan>& out,
+                std::string& err);
+// Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
+// and fills perm/phases/unit if every row and column holds exactly one nonzero.
+int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);
+}  // namespace iqb
+#endif

@@ -1,0 +1,249 @@
+// plan_emulator.cpp -- TEST ONLY.  Executes the passes planned by
+// invariantq_b200/csrc/iq_sched.cpp on the CPU with the semantics of
+// tile_pass_kernel (iq_kernels.cu): tensor-map box copies computed from the
+// shared addressing helpers in iq_plan.h, register stages with octet lanes,
+// and every operation kind.  It lets the CPU test suite check the scheduler,
+// the descriptor encoding and the tile addressing against the oracle.  It also
+// checks that the box copies of a pass cover every amplitude exactly once.
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../invariantq_b200/csrc/iq_plan.h"
+
+using namespace iqb;
+using cd = std::complex<double>;
+
+namespace {
+
+struct Emu {
+  int nbits;
+  std::vector<cd> pool;
+  cd* state;
+  std::string err;
+
+  cd mat(uint32_t off, int i) const { return pool[off + i]; }
+
+  bool copy_tile(const PassDesc& P, uint64_t t, std::vector<cd>& tile, bool load, std::vector<uint8_t>& seen) {
+    uint64_t gd[5], gs[4];
+    uint32_t box[5];
+    pass_tmap_layout(P, nbits, gd, gs, box);
+    const uint64_t base = tile_base(t, P);
+    const int nissue = 1 << (P.nH - P.nbox);
+    const uint32_t box_elems = 1u << (P.c + P.nbox);
+    double* sd = reinterpret_cast<double*>(state);
+    double* td = reinterpret_cast<double*>(tile.data());
+    for (int j = 0; j < nissue; ++j) {
+      int c[5];
+      c[0] = 0;
+      chunk_coords(base | issue_offset(j, P), P, c[1], c[2], c[3], c[4]);
+      for (int d = 1; d < 5; ++d)
+        if (c[d] < 0 || (uint64_t)c[d] + box[d] > gd[d]) { err = "box out of tensor bounds"; return false; }
+      uint64_t lin = 0;
+      for (uint32_t i4 = 0; i4 < box[4]; ++i4)
+        for (uint32_t i3 = 0; i3 < box[3]; ++i3)
+          for (uint32_t i2 = 0; i2 < box[2]; ++i2)
+            for (uint32_t i1 = 0; i1 < box[1]; ++i1)
+              for (uint32_t i0 = 0; i0 < box[0]; ++i0, ++lin) {
+                const uint64_t g = (uint64_t)(c[0] + i0) * 8 + (uint64_t)(c[1] + i1) * gs[0] +
+                                   (uint64_t)(c[2] + i2) * gs[1] + (uint64_t)(c[3] + i3) * gs[2] +
+                                   (uint64_t)(c[4] + i4) * gs[3];
+                if (g % 8) { err = "misaligned element"; return false; }
+                const uint64_t gi = g / 8;
+                if (gi >= (2ull << nbits)) { err = "global address out of range"; return false; }
+                const uint64_t si = (uint64_t)j * box_elems * 2 + lin;
+                if (si >= tile.size() * 2) { err = "shared address out of range"; return false; }
+                if (load) {
+                  td[si] = sd[gi];
+                  if (gi % 2 == 0) {
+                    if (seen[gi / 2]) { err = "amplitude loaded twice in one pass"; return false; }
+                    seen[gi / 2] = 1;
+                  }
+                } else {
+                  sd[gi] = td[si];
+                }
+              }
+    }
+    return true;
+  }
+
+  // one stage: 2^nt octet-subcubes, 8 lanes each, 2^R registers per lane
+  bool run_stage(const PassDesc& P, int s, std::vector<cd>& tile) {
+    const StageDesc& sd = P.st[s];
+    const int R = P.R, NV = 1 << R;
+    auto voff = [&](int v) {
+      uint32_t o = 0;
+      for (int i = 0; i < R; ++i)
+        if ((v >> i) & 1) o |= 1u << sd.S[i];
+      return o;
+    };
+    for (uint32_t u = 0; u < (1u << sd.nt); ++u) {
+      uint32_t ub = 0;
+      for (int i = 0; i < sd.nt; ++i) ub |= ((u >> i) & 1u) << sd.tb[i];
+      std::vector<std::vector<cd>> a(8, std::vector<cd>(NV));
+      uint32_t base[8];
+      for (int L = 0; L < 8; ++L) {
+        base[L] = ub | ((L & 1u) << sd.lane[0]) | (((L >> 1) & 1u) << sd.lane[1]) | (((L >> 2) & 1u) << sd.lane[2]);
+        for (int v = 0; v < NV; ++v) a[L][v] = tile[base[L] | voff(v)];
+      }
+      bool stored = false;
+      for (int o = sd.op0; o < sd.op1; ++o) {
+        const OpDesc& od = P.ops[o];
+        const bool unit = od.flags & OPF_UNIT_PHASE;
+        switch (od.kind) {
+          case OP_D1R:
+            for (int L = 0; L < 8; ++L)
+              for (int v = 0; v < NV; ++v) {
+                if (v & (1 << od.a)) continue;
+                const cd x = a[L][v], y = a[L][v | (1 << od.a)];
+                a[L][v] = mat(od.mat, 0) * x + mat(od.mat, 1) * y;
+                a[L][v | (1 << od.a)] = mat(od.mat, 2) * x + mat(od.mat, 3) * y;
+              }
+            break;
+          case OP_D1L: {
+            auto old = a;
+            for (int L = 0; L < 8; ++L) {
+              const int my = (L >> od.a) & 1, pl = L ^ (1 << od.a);
+              for (int v = 0; v < NV; ++v)
+                a[L][v] = (my ? mat(od.mat, 3) : mat(od.mat, 0)) * old[L][v] +
+                          (my ? mat(od.mat, 2) : mat(od.mat, 1)) * old[pl][v];
+            }
+            break;
+          }
+          case OP_M1R:
+            for (int L = 0; L < 8; ++L)
+              for (int v = 0; v < NV; ++v) {
+                if (v & (1 << od.a)) continue;
+                cd x = a[L][v], y = a[L][v | (1 << od.a)];
+                if (od.perm & 1) std::swap(x, y);
+                if (!unit) { x *= mat(od.mat, 0); y *= mat(od.mat, 1); }
+                a[L][v] = x;
+                a[L][v | (1 << od.a)] = y;
+              }
+            break;
+          case OP_M1L: {
+            auto old = a;
+            for (int L = 0; L < 8; ++L) {
+              const int my = (L >> od.a) & 1, pl = L ^ (1 << od.a);
+              for (int v = 0; v < NV; ++v) {
+                cd x = (od.perm & 1) ? old[pl][v] : old[L][v];
+                a[L][v] = unit ? x : mat(od.mat, my) * x;
+              }
+            }
+            break;
+          }
+          case OP_D2R:
+          case OP_M2R:
+            for (int L = 0; L < 8; ++L)
+              for (int v = 0; v < NV; ++v) {
+                if (v & ((1 << od.a) | (1 << od.b))) continue;
+                int idx[4];
+                cd x[4];
+                for (int m = 0; m < 4; ++m) {
+                  idx[m] = v | ((m & 1) << od.a) | (((m >> 1) & 1) << od.b);
+                  x[m] = a[L][idx[m]];
+                }
+                for (int r = 0; r < 4; ++r) {
+                  cd acc;
+                  if (od.kind == OP_D2R) {
+                    acc = 0.0;
+                    for (int m = 0; m < 4; ++m) acc += mat(od.mat, 4 * r + m) * x[m];
+                  } else {
+                    acc = x[(od.perm >> (2 * r)) & 3];
+                    if (!unit) acc *= mat(od.mat, r);
+                  }
+                  a[L][idx[r]] = acc;
+                }
+              }
+            break;
+          case OP_DKR: {
+            const int k = od.k, D = 1 << k;
+            if (o != sd.op1 - 1) { err = "dense block is not the last operation of its stage"; return false; }
+            for (int L = 0; L < 8; ++L)
+              for (int g = 0; g < NV; g += D)
+                for (int r = 0; r < D; ++r) {
+                  cd acc = 0.0;
+                  for (int cc = 0; cc < D; ++cc) acc += mat(od.mat, r * D + cc) * a[L][g + cc];
+                  tile[base[L] | voff(g + r)] = acc;
+                }
+            stored = true;
+            break;
+          }
+          default:
+            err = "unknown operation kind";
+            return false;
+        }
+      }
+      if (!stored)
+        for (int L = 0; L < 8; ++L)
+          for (int v = 0; v < NV; ++v) tile[base[L] | voff(v)] = a[L][v];
+    }
+    return true;
+  }
+};
+
+}  // namespace
+
+extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double budget, int nops, const int* ks,
+                         const int* qs, const double* mats, const long long* mat_off, double* state_il,
+                         int* npasses, int* ops_per_pass, char* errbuf, int errlen) {
+  Emu e;
+  e.nbits = nbits;
+  e.state = reinterpret_cast<cd*>(state_il);
+  std::vector<SchedOp> ops;
+  for (int i = 0; i < nops; ++i) {
+    SchedOp o{};
+    o.k = (uint8_t)ks[i];
+    for (int j = 0; j < ks[i]; ++j) o.q[j] = (uint8_t)qs[i * 5 + j];
+    const int d = 1 << ks[i];
+    const double* m = mats + 2 * mat_off[i];
+    o.mat = (uint32_t)e.pool.size();
+    for (int j = 0; j < d * d; ++j) e.pool.emplace_back(m[2 * j], m[2 * j + 1]);
+    double ph[8];
+    uint8_t perm = 0, unit = 0;
+    if (ks[i] <= 2 && classify_monomial(m, ks[i], &perm, ph, &unit)) {
+      o.mono = 1;
+      o.perm = perm;
+      o.unit = unit;
+      o.mat = (uint32_t)e.pool.size();
+      for (int j = 0; j < d; ++j) e.pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    }
+    ops.push_back(o);
+  }
+  SchedParams p{};
+  p.nbits = nbits;
+  p.M = M;
+  p.c = c;
+  p.R = R;
+  p.max_stages = max_stages;
+  p.budget = budget;
+  std::vector<PassPlan> plans;
+  std::string err;
+  if (plan_passes(p, ops, plans, err) < 0) {
+    snprintf(errbuf, errlen, "plan: %s", err.c_str());
+    return -1;
+  }
+  *npasses = (int)plans.size();
+  for (size_t pi = 0; pi < plans.size(); ++pi) {
+    const PassDesc& P = plans[pi].desc;
+    if (ops_per_pass) ops_per_pass[pi] = plans[pi].nsrc;
+    std::vector<cd> tile((size_t)1 << P.M);
+    std::vector<uint8_t> seen((size_t)1 << nbits, 0);
+    for (uint64_t t = 0; t < P.ntiles; ++t) {
+      if (!e.copy_tile(P, t, tile, true, seen)) break;
+      for (int s = 0; s < P.nstages && e.err.empty(); ++s) e.run_stage(P, s, tile);
+      if (!e.err.empty()) break;
+      if (!e.copy_tile(P, t, tile, false, seen)) break;
+    }
+    if (e.err.empty())
+      for (size_t i = 0; i < seen.size(); ++i)
+        if (!seen[i]) { e.err = "amplitude not covered by a pass"; break; }
+    if (!e.err.empty()) {
+      snprintf(errbuf, errlen, "pass %zu: %s", pi, e.err.c_str());
+      return -1;
+    }
+  }
+  return 0;
+}
