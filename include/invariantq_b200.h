@@ -140,9 +140,20 @@ size_t iq_statevector_num_qubits(void* sv);
 int iq_handle_set_option(void* h, const char* key, double value);
 double iq_handle_get_option(void* h, const char* key);
 /* Counters: out[0] passes, [1] operations applied, [2] algorithmic bytes moved by
- * passes, [3] kernel launches, [4] flushes, [5] tile-pass launches.  Returns the
- * number of values written. */
+ * passes, [3] kernel launches, [4] flushes, [5] tile-pass launches, [6] bytes of
+ * operation matrices copied host->device by flushes.  Returns the number of
+ * values written. */
 int iq_handle_stats(void* h, double* out, size_t n);
+/* Recorded programs: operations issued between record_begin and record_end are
+ * planned once into tile passes whose matrices and descriptors stay on the
+ * device; program_run launches them on the handle's stream (any number of
+ * times, on the handle's current amplitudes).  program_info: out[0] passes,
+ * [1] operations, [2] matrix bytes, [3] planned arithmetic cost. */
+int   iq_handle_record_begin(void* h);
+void* iq_handle_record_end(void* h);
+int   iq_handle_program_run(void* h, void* prog);
+int   iq_program_info(void* prog, double* out, size_t n);
+void  iq_program_free(void* prog);
 /* With option "profile" = 1 every tile pass is bracketed by CUDA events; this
  * returns up to max per-pass durations in ms (oldest first) and clears them. */
 int iq_handle_profile_read(void* h, double* ms_out, size_t max);

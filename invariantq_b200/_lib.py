@@ -92,6 +92,11 @@ SIGNATURES = {
     "iq_handle_get_option": ([_v, ctypes.c_char_p], _d),
     "iq_handle_stats": ([_v, c_dp, _sz], _i),
     "iq_handle_profile_read": ([_v, c_dp, _sz], _i),
+    "iq_handle_record_begin": ([_v], _i),
+    "iq_handle_record_end": ([_v], _v),
+    "iq_handle_program_run": ([_v, _v], _i),
+    "iq_program_info": ([_v, c_dp, _sz], _i),
+    "iq_program_free": ([_v], None),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),
     "iq_density_matrix_get_diagonal": ([_v, c_dp], None),

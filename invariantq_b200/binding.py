@@ -45,15 +45,59 @@ class _Handle:
         return self._lib.iq_handle_get_option(self._ptr, key.encode())
 
     def stats(self) -> Dict[str, float]:
-        out = np.zeros(6)
-        self._lib.iq_handle_stats(self._ptr, _p(out), 6)
-        keys = ("passes", "ops", "bytes", "launches", "flushes", "tile_passes")
+        out = np.zeros(7)
+        self._lib.iq_handle_stats(self._ptr, _p(out), 7)
+        keys = ("passes", "ops", "bytes", "launches", "flushes", "tile_passes", "h2d_bytes")
         return dict(zip(keys, out.tolist()))
+
+    def record(self):
+        """Context manager: operations issued inside become a device-resident
+        ``Program`` (planned once, replayed with ``run``)."""
+        return _Recorder(self)
 
     def profile_read(self, max_items: int = 1 << 16) -> np.ndarray:
         out = np.zeros(max_items)
         n = self._lib.iq_handle_profile_read(self._ptr, _p(out), max_items)
         return out[:n].copy()
+
+
+class Program:
+    """Planned tile passes + matrices resident on the device (iq_handle_record_end)."""
+
+    def __init__(self, handle: "_Handle", ptr: int):
+        self._lib = handle._lib
+        self._ptr = ptr
+        out = np.zeros(4)
+        self._lib.iq_program_info(ptr, _p(out), 4)
+        self.passes, self.ops, self.matrix_bytes, self.planned_cost = int(out[0]), int(out[1]), out[2], out[3]
+
+    def run(self, handle: "_Handle") -> None:
+        if self._lib.iq_handle_program_run(handle._ptr, self._ptr) != 0:
+            check(self._lib)
+
+    def __del__(self):
+        if getattr(self, "_ptr", None):
+            self._lib.iq_program_free(self._ptr)
+            self._ptr = None
+
+
+class _Recorder:
+    def __init__(self, h: "_Handle"):
+        self.h = h
+        self.program = None
+
+    def __enter__(self):
+        if self.h._lib.iq_handle_record_begin(self.h._ptr) != 0:
+            check(self.h._lib)
+        return self
+
+    def __exit__(self, et, ev, tb):
+        p = self.h._lib.iq_handle_record_end(self.h._ptr)
+        if not p:
+            check(self.h._lib)
+            raise RuntimeError("recording failed")
+        self.program = Program(self.h, p)
+        return False
 
 
 class NativeStateVector(_Handle):

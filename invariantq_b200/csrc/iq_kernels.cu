@@ -94,15 +94,27 @@ __device__ __forceinline__ void bulk_wait_read_all() {
 }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-constexpr uint32_t kSpinLimit = 1u << 22;
+// Wait limit of one mbarrier phase: 2 s of %globaltimer (a tile load or a
+// consumer stage takes microseconds).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Bounded wait on an mbarrier phase.  Returns false (and raises the abort flag
-// plus the status word) when the limit runs out, or immediately once aborted.
+// plus the status word) when the limit runs out, or as soon as another thread
+// of the CTA has aborted.
 __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                              int* status, int code) {
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
+    if (global_ns() - t0 > kWaitLimitNs) break;
   }
   *abort_flag = 1;
   atomicCAS(status, 0, code);

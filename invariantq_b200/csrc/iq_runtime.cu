@@ -198,7 +198,8 @@ struct Engine {
   int profile = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
 
-  double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0;
+  double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0, st_h2d = 0;
+  bool recording = false;
 
   bool init(int kind_, size_t n) {
     kind = kind_;
@@ -271,9 +272,7 @@ struct Engine {
   bool select() { return cuda_ok(cudaSetDevice(device), "cudaSetDevice"); }
 
   bool reset_state() {
-    ops.clear();
-    dense_off.clear();
-    pool.clear();
+    if (!recording) clear_queue();
     ++st_launches;
     ++g_launches;
     return cuda_ok(launch_set_basis(d_state, dim, stream), "reset");
@@ -322,7 +321,7 @@ struct Engine {
     }
     ops.push_back(o);
     dense_off.push_back(dense);
-    if ((int)ops.size() >= flush_ops) return flush();
+    if (!recording && (int)ops.size() >= flush_ops) return flush();
     return true;
   }
 
@@ -361,74 +360,118 @@ struct Engine {
     return true;
   }
 
-  bool flush() {
-    if (ops.empty()) return true;
-    if (!select()) return false;
-    if (!upload_pool()) return false;
-    ++st_flushes;
-    bool ok = true;
+  // A planned batch of queued operations: pass descriptors + encoded tensor
+  // maps (tile path) or per-op launches (simple path), with the matrix pool
+  // on the device.  flush() builds a transient one over the per-handle pool
+  // buffer; record_end() builds one that owns its device buffer.
+  struct Program {
+    bool tiled = false;
+    std::vector<PassPlan> plans;
+    std::vector<CUtensorMap> tmaps;
+    std::vector<SimpleOp> sops;
+    double2* d_mats = nullptr;   // owned when `owns` is set
+    bool owns = false;
+    size_t pool_elems = 0;
+    int nops = 0;
+  };
+
+  bool build_program(Program& pg, bool own) {
+    pg.nops = (int)ops.size();
+    pg.pool_elems = pool.size();
+    if (own) {
+      if (!pool.empty()) {
+        if (!cuda_ok(cudaMalloc(&pg.d_mats, pool.size() * sizeof(double2)), "cudaMalloc program matrices"))
+          return false;
+        pg.owns = true;
+        if (!cuda_ok(cudaMemcpy(pg.d_mats, pool.data(), pool.size() * sizeof(double2), cudaMemcpyHostToDevice),
+                     "H2D program matrices"))
+          return false;
+      }
+    } else {
+      if (!upload_pool()) return false;
+      pg.d_mats = d_pool;
+    }
     int maxk = 1;
     for (auto& o : ops) maxk = std::max<int>(maxk, o.k);
-    const bool tiled = !eager && nbits >= 7;
-    if (!tiled) {
-      for (size_t i = 0; i < ops.size() && ok; ++i) {
+    pg.tiled = !eager && nbits >= 7;
+    if (!pg.tiled) {
+      for (size_t i = 0; i < ops.size(); ++i) {
         SimpleOp so{};
         so.k = ops[i].k;
         for (int j = 0; j < so.k; ++j) so.q[j] = ops[i].q[j];
         so.mat = dense_off[i];
-        ok = cuda_ok(launch_simple_op(d_state, nbits, so, d_pool, stream), "simple gate kernel");
-        ++st_launches;
-        ++g_launches;
-        st_passes += 1;
-        st_bytes += 32.0 * (double)dim;
+        pg.sops.push_back(so);
       }
-      st_ops += (double)ops.size();
-    } else {
-      SchedParams p = sp;
-      p.nbits = nbits;
-      p.R = maxk > 4 ? 5 : 4;
-      std::vector<PassPlan> plans;
-      std::string err;
-      if (plan_passes(p, ops, plans, err) < 0) {
-        set_error(E_STATE, "scheduler: %s", err.c_str());
-        ops.clear();
-        dense_off.clear();
-        pool.clear();
+      return true;
+    }
+    SchedParams p = sp;
+    p.nbits = nbits;
+    p.R = maxk > 4 ? 5 : 4;
+    std::string err;
+    if (plan_passes(p, ops, pg.plans, err) < 0) {
+      set_error(E_STATE, "scheduler: %s", err.c_str());
+      return false;
+    }
+    pg.tmaps.resize(pg.plans.size());
+    char emsg[256];
+    for (size_t i = 0; i < pg.plans.size(); ++i)
+      if (encode_pass_tmap(&pg.tmaps[i], d_state, nbits, pg.plans[i].desc, emsg, sizeof(emsg)) != 0) {
+        set_error(E_CUDA, "%s", emsg);
         return false;
       }
-      char emsg[256];
-      for (auto& pl : plans) {
-        alignas(64) CUtensorMap tm;
-        if (encode_pass_tmap(&tm, d_state, nbits, pl.desc, emsg, sizeof(emsg)) != 0) {
-          set_error(E_CUDA, "%s", emsg);
-          ok = false;
-          break;
-        }
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        if (profile) {
-          cudaEventCreate(&e0);
-          cudaEventCreate(&e1);
-          cudaEventRecord(e0, stream);
-        }
-        if (!cuda_ok(launch_tile_pass(tm, pl.desc, d_pool, d_status, tl, num_sms, stream), "tile pass kernel")) {
-          ok = false;
-          break;
-        }
-        if (profile) {
-          cudaEventRecord(e1, stream);
-          prof.emplace_back(e0, e1);
-        }
+    return true;
+  }
+
+  bool run_program(const Program& pg) {
+    if (!pg.tiled) {
+      for (auto& so : pg.sops) {
+        if (!cuda_ok(launch_simple_op(d_state, nbits, so, pg.d_mats, stream), "simple gate kernel")) return false;
         ++st_launches;
         ++g_launches;
-        ++st_tile;
         st_passes += 1;
         st_bytes += 32.0 * (double)dim;
-        st_ops += pl.nsrc;
       }
+      st_ops += (double)pg.sops.size();
+      return true;
     }
+    for (size_t i = 0; i < pg.plans.size(); ++i) {
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (profile) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, stream);
+      }
+      if (!cuda_ok(launch_tile_pass(pg.tmaps[i], pg.plans[i].desc, pg.d_mats, d_status, tl, num_sms, stream),
+                   "tile pass kernel"))
+        return false;
+      if (profile) {
+        cudaEventRecord(e1, stream);
+        prof.emplace_back(e0, e1);
+      }
+      ++st_launches;
+      ++g_launches;
+      ++st_tile;
+      st_passes += 1;
+      st_bytes += 32.0 * (double)dim;
+      st_ops += pg.plans[i].nsrc;
+    }
+    return true;
+  }
+
+  void clear_queue() {
     ops.clear();
     dense_off.clear();
     pool.clear();
+  }
+
+  bool flush() {
+    if (ops.empty() || recording) return true;
+    if (!select()) return false;
+    ++st_flushes;
+    st_h2d += (double)pool.size() * sizeof(double2);
+    Program pg;
+    const bool ok = build_program(pg, false) && run_program(pg);
+    clear_queue();
     return ok;
   }
 
@@ -1035,8 +1078,8 @@ double iq_handle_get_option(void* h, const char* key) {
 int iq_handle_stats(void* h, double* out, size_t n) {
   Engine* e = static_cast<Engine*>(h);
   if (!e || !out) return 0;
-  const double v[6] = {e->st_passes, e->st_ops, e->st_bytes, e->st_launches, e->st_flushes, e->st_tile};
-  const size_t m = std::min<size_t>(n, 6);
+  const double v[7] = {e->st_passes, e->st_ops, e->st_bytes, e->st_launches, e->st_flushes, e->st_tile, e->st_h2d};
+  const size_t m = std::min<size_t>(n, 7);
   for (size_t i = 0; i < m; ++i) out[i] = v[i];
   return (int)m;
 }
@@ -1057,6 +1100,62 @@ int iq_handle_profile_read(void* h, double* ms_out, size_t max) {
   }
   e->prof.clear();
   return (int)n;
+}
+
+// ============================================================ recorded programs
+
+int iq_handle_record_begin(void* h) {
+  Engine* e = static_cast<Engine*>(h);
+  if (!e || !e->flush()) return -1;
+  e->recording = true;
+  return 0;
+}
+
+void* iq_handle_record_end(void* h) {
+  Engine* e = static_cast<Engine*>(h);
+  if (!e) return nullptr;
+  if (!e->recording) {
+    set_error(E_STATE, "record_end without record_begin");
+    return nullptr;
+  }
+  e->recording = false;
+  if (!e->select()) return nullptr;
+  auto* pg = new Engine::Program();
+  if (!e->build_program(*pg, true)) {
+    if (pg->d_mats && pg->owns) cudaFree(pg->d_mats);
+    delete pg;
+    e->clear_queue();
+    return nullptr;
+  }
+  e->clear_queue();
+  return pg;
+}
+
+int iq_handle_program_run(void* h, void* prog) {
+  Engine* e = static_cast<Engine*>(h);
+  auto* pg = static_cast<Engine::Program*>(prog);
+  if (!e || !pg) return -1;
+  if (!e->flush() || !e->select()) return -1;
+  return e->run_program(*pg) ? 0 : -1;
+}
+
+int iq_program_info(void* prog, double* out, size_t n) {
+  auto* pg = static_cast<Engine::Program*>(prog);
+  if (!pg || !out) return 0;
+  double planned_cost = 0.0;
+  for (auto& p : pg->plans) planned_cost += p.cost;
+  const double v[4] = {(double)(pg->tiled ? pg->plans.size() : pg->sops.size()), (double)pg->nops,
+                       (double)pg->pool_elems * sizeof(double2), planned_cost};
+  const size_t m = std::min<size_t>(n, 4);
+  for (size_t i = 0; i < m; ++i) out[i] = v[i];
+  return (int)m;
+}
+
+void iq_program_free(void* prog) {
+  auto* pg = static_cast<Engine::Program*>(prog);
+  if (!pg) return;
+  if (pg->owns && pg->d_mats) cudaFree(pg->d_mats);
+  delete pg;
 }
 
 // ============================================================ density matrix

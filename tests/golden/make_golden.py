@@ -308,6 +308,14 @@ def gen_simulators(iq, out):
     np.savez_compressed(out / "simulators.npz", **d)
 
 
+def gen_symbols(ref_dir: Path, out: Path):
+    """The exported function names of the reference C ABI (core/include/c_api.h)."""
+    import re
+    text = (ref_dir / "core" / "include" / "c_api.h").read_text()
+    names = re.findall(r"\b(iq_[a-z0-9_]+)\s*\(", text)
+    (out / "c_api_symbols.txt").write_text("\n".join(names) + "\n")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -321,6 +329,7 @@ def main():
         gen_dm_ops(iq, binding, out)
         gen_gates(iq, out)
         gen_simulators(iq, out)
+    gen_symbols(Path(a.reference), out)
     for f in sorted(out.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
