@@ -34,6 +34,7 @@ constexpr int kLaneBits = 3;       // octet = 8 lanes
 constexpr int kMaxStages = 24;
 constexpr int kMaxPassOps = 160;
 constexpr int kMaxK = 5;           // widest dense block the kernels apply
+constexpr int kSmemMatElems = 1024; // per-pass matrix block kept in shared memory (16 KiB)
 
 enum OpKind : uint8_t {
   OP_NONE = 0,
@@ -74,6 +75,8 @@ struct PassDesc {
   uint8_t H[kMaxTileBits + 3];   // physical bit of tile-local bit c + i (ascending)
   uint64_t ntiles;
   uint32_t nops, pad2;
+  uint32_t mat_base;             // this pass's matrix block in the flush's matrix pool
+  uint32_t mat_elems;            // complex elements in the block (ops' `mat` are relative to it)
   StageDesc st[kMaxStages];
   OpDesc ops[kMaxPassOps];
 };
@@ -86,6 +89,7 @@ struct SchedOp {
   uint8_t perm;          // monomial permutation (see OpDesc)
   uint8_t unit;          // monomial with unit phases
   uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
+  uint32_t dense;        // complex offset of the dense 2^k x 2^k matrix (always present)
 };
 
 struct SchedParams {
@@ -130,58 +134,65 @@ IQ_HD uint64_t issue_offset(int j, const PassDesc& P) {
   return off;
 }
 
+// Shared-memory slot of tile-local amplitude j: the 128-byte TMA swizzle XORs
+// bits 0..2 of the 16-byte unit index with bits 3..5.  The map is linear over
+// XOR, so slot(a ^ b) = slot(a) ^ slot(b) for any two indices.
+IQ_HD uint32_t swz(uint32_t j) { return j ^ ((j >> 3) & 7u); }
+
 // 5-D view of the array used by the pass tensor map (dimension 0 innermost,
 // counted in doubles; strides in bytes for dimensions 1..4).  The bits of the
 // amplitude index are cut at the first two tile bits H[0], H[1]:
-//   dim0 = the 2^c-amplitude chunk, dim1 = bits [c, H0), dim2 = bit H0,
-//   dim3 = bits (H0, H1), dim4 = bits [H1, nbits).
-// The box takes the whole chunk and both values of H0 and H1, so one copy
-// moves 2^(c + nbox) amplitudes; the other tile bits are enumerated by issues.
+//   dim0 = 8 amplitudes (128 B, the swizzle span), dim1 = bits [3, H0),
+//   dim2 = bit H0, dim3 = bits (H0, H1), dim4 = bits [H1, nbits).
+// The box takes 2^(c-3) rows of dim1 (the rest of the 2^c chunk) and both
+// values of H0 and H1, so one copy moves 2^(c + nbox) amplitudes; the other
+// tile bits are enumerated by issues.
 IQ_HD void pass_tmap_layout(const PassDesc& d, int nbits, uint64_t gd[5], uint64_t gs[4], uint32_t box[5]) {
   const int c = d.c;
   const uint64_t E = 16;
-  const uint64_t inner = 2ull << c;
   const uint64_t top = (1ull << nbits) * E;
+  gd[0] = 16;
+  gs[0] = 8 * E;
+  box[0] = 16;
+  box[1] = 1u << (c - 3);
   if (d.nbox == 2) {
     const int h0 = d.H[0], h1 = d.H[1];
-    gd[0] = inner; gd[1] = 1ull << (h0 - c); gd[2] = 2; gd[3] = 1ull << (h1 - h0 - 1); gd[4] = 1ull << (nbits - h1);
-    gs[0] = (1ull << c) * E; gs[1] = (1ull << h0) * E; gs[2] = (1ull << (h0 + 1)) * E; gs[3] = (1ull << h1) * E;
-    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 2; box[3] = 1; box[4] = 2;
+    gd[1] = 1ull << (h0 - 3); gd[2] = 2; gd[3] = 1ull << (h1 - h0 - 1); gd[4] = 1ull << (nbits - h1);
+    gs[1] = (1ull << h0) * E; gs[2] = (1ull << (h0 + 1)) * E; gs[3] = (1ull << h1) * E;
+    box[2] = 2; box[3] = 1; box[4] = 2;
   } else if (d.nbox == 1) {
     const int h0 = d.H[0];
-    gd[0] = inner; gd[1] = 1ull << (h0 - c); gd[2] = 1ull << (nbits - h0); gd[3] = 1; gd[4] = 1;
-    gs[0] = (1ull << c) * E; gs[1] = (1ull << h0) * E; gs[2] = top; gs[3] = top;
-    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 2; box[3] = 1; box[4] = 1;
+    gd[1] = 1ull << (h0 - 3); gd[2] = 1ull << (nbits - h0); gd[3] = 1; gd[4] = 1;
+    gs[1] = (1ull << h0) * E; gs[2] = top; gs[3] = top;
+    box[2] = 2; box[3] = 1; box[4] = 1;
   } else {
-    gd[0] = inner; gd[1] = 1ull << (nbits - c); gd[2] = 1; gd[3] = 1; gd[4] = 1;
-    gs[0] = (1ull << c) * E; gs[1] = top; gs[2] = top; gs[3] = top;
-    box[0] = (uint32_t)inner; box[1] = 1; box[2] = 1; box[3] = 1; box[4] = 1;
+    gd[1] = 1ull << (nbits - 3); gd[2] = 1; gd[3] = 1; gd[4] = 1;
+    gs[1] = top; gs[2] = top; gs[3] = top;
+    box[2] = 1; box[3] = 1; box[4] = 1;
   }
 }
 
-// Tensor-map coordinates (dims 1..4) of the copy whose first amplitude is A.
+// Tensor-map coordinates (dims 1..4) of the copy whose first amplitude is A
+// (A has zeros in bits [0, c) and at the box bits).
 IQ_HD void chunk_coords(uint64_t A, const PassDesc& P, int& c1, int& c2, int& c3, int& c4) {
-  const int c = P.c;
   if (P.nbox == 2) {
     const int h0 = P.H[0], h1 = P.H[1];
-    c1 = (int)((A >> c) & ((1ULL << (h0 - c)) - 1));
+    c1 = (int)((A >> 3) & ((1ULL << (h0 - 3)) - 1));
     c2 = 0;
     c3 = (int)((A >> (h0 + 1)) & ((1ULL << (h1 - h0 - 1)) - 1));
     c4 = (int)(A >> h1);
   } else if (P.nbox == 1) {
     const int h0 = P.H[0];
-    c1 = (int)((A >> c) & ((1ULL << (h0 - c)) - 1));
+    c1 = (int)((A >> 3) & ((1ULL << (h0 - 3)) - 1));
     c2 = (int)(A >> h0);
     c3 = 0;
     c4 = 0;
   } else {
-    c1 = (int)(A >> c);
+    c1 = (int)(A >> 3);
     c2 = c3 = c4 = 0;
   }
 }
 
-// Plan passes for ops[0..nops): returns the number of passes written to out
-// (growing the vector), or -1 with a message in err on failure.
 }  // namespace iqb
 
 #ifdef __cplusplus
@@ -190,6 +201,17 @@ IQ_HD void chunk_coords(uint64_t A, const PassDesc& P, int& c1, int& c2, int& c3
 namespace iqb {
 int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vector<PassPlan>& out,
                 std::string& err);
+struct cplx64 { double re, im; };
+// Fuse runs of queued operations on at most two qubits into single 4x4 blocks
+// (a two-qubit operation absorbs the open one-qubit blocks of its qubits and
+// later one-qubit operations on them), appending the fused matrices to `pool`.
+// Operation order per qubit is preserved.  Returns the fused list.
+std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool);
+// Re-pack the matrix data each pass references (absolute offsets into `pool`)
+// into one contiguous block per pass: sets desc.mat_base / mat_elems and makes
+// every op's `mat` relative to its pass block, which the kernel stages in
+// shared memory.
+void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::vector<cplx64>& packed);
 // Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
 // and fills perm/phases/unit if every row and column holds exactly one nonzero.
 int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);

@@ -174,8 +174,7 @@ struct Engine {
   cudaStream_t stream = nullptr;
 
   std::vector<SchedOp> ops;
-  std::vector<uint32_t> dense_off;   // dense matrix offset per queued op (simple path)
-  std::vector<double2> pool;
+  std::vector<cplx64> pool;          // matrices of the queued ops (dense, plus phases of monomials)
 
   double2* d_pool = nullptr;
   size_t d_pool_cap = 0;
@@ -194,6 +193,7 @@ struct Engine {
   SchedParams sp{};
   TileLaunch tl{};
   int eager = 0;
+  int fuse = 1;
   int flush_ops = 4096;
   int profile = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
@@ -237,13 +237,14 @@ struct Engine {
     if (!cuda_ok(cudaEventCreateWithFlags(&pool_ev, cudaEventDisableTiming), "cudaEventCreate")) return false;
     cudaMemsetAsync(d_status, 0, sizeof(int), stream);
     sp.nbits = nbits;
-    sp.M = env_int("IQ_TILE_BITS", 12);
+    tl.consumers = env_int("IQ_CONSUMERS", 128);
+    sp.M = env_int("IQ_TILE_BITS", tl.consumers >= 256 ? 12 : 11);
     sp.c = env_int("IQ_CHUNK_BITS", 5);
     sp.R = 4;
     sp.max_stages = env_int("IQ_MAX_STAGES", 8);
     sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
-    tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 1);
+    tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", tl.consumers >= 256 ? 1 : 2);
     eager = env_int("IQ_EAGER", 0);
     return reset_state();
   }
@@ -305,8 +306,9 @@ struct Engine {
     o.k = (uint8_t)k;
     for (int i = 0; i < k; ++i) o.q[i] = (uint8_t)q[i];
     const uint32_t dense = (uint32_t)pool.size();
-    for (int i = 0; i < d * d; ++i) pool.push_back(make_double2(m[i].real(), m[i].imag()));
+    for (int i = 0; i < d * d; ++i) pool.push_back({m[i].real(), m[i].imag()});
     o.mat = dense;
+    o.dense = dense;
     o.mono = 0;
     if (k <= 2) {
       double ph[8];
@@ -316,17 +318,16 @@ struct Engine {
         o.perm = perm;
         o.unit = unit;
         o.mat = (uint32_t)pool.size();
-        for (int i = 0; i < d; ++i) pool.push_back(make_double2(ph[2 * i], ph[2 * i + 1]));
+        for (int i = 0; i < d; ++i) pool.push_back({ph[2 * i], ph[2 * i + 1]});
       }
     }
     ops.push_back(o);
-    dense_off.push_back(dense);
     if (!recording && (int)ops.size() >= flush_ops) return flush();
     return true;
   }
 
-  bool upload_pool() {
-    const size_t n = pool.size();
+  // copy `n` complex values to the per-handle device pool through the pinned buffer
+  bool upload_pool(const double2* src, size_t n) {
     if (n == 0) return true;
     if (n > d_pool_cap) {
       if (d_pool) {
@@ -352,11 +353,12 @@ struct Engine {
     } else if (pool_ev_recorded) {
       cudaEventSynchronize(pool_ev);   // previous copy out of h_pool has finished
     }
-    memcpy(h_pool, pool.data(), n * sizeof(double2));
+    memcpy(h_pool, src, n * sizeof(double2));
     if (!cuda_ok(cudaMemcpyAsync(d_pool, h_pool, n * sizeof(double2), cudaMemcpyHostToDevice, stream), "H2D matrices"))
       return false;
     cudaEventRecord(pool_ev, stream);
     pool_ev_recorded = true;
+    st_h2d += (double)n * sizeof(double2);
     return true;
   }
 
@@ -377,48 +379,54 @@ struct Engine {
 
   bool build_program(Program& pg, bool own) {
     pg.nops = (int)ops.size();
-    pg.pool_elems = pool.size();
-    if (own) {
-      if (!pool.empty()) {
-        if (!cuda_ok(cudaMalloc(&pg.d_mats, pool.size() * sizeof(double2)), "cudaMalloc program matrices"))
+    const std::vector<SchedOp> fused = fuse ? fuse_two_qubit_blocks(ops, pool) : ops;
+    int maxk = 1;
+    for (auto& o : fused) maxk = std::max<int>(maxk, o.k);
+    pg.tiled = !eager && nbits >= 7;
+    std::vector<cplx64> packed;
+    const cplx64* src = pool.data();
+    size_t nsrc = pool.size();
+    if (!pg.tiled) {
+      for (const SchedOp& o : fused) {
+        SimpleOp so{};
+        so.k = o.k;
+        for (int j = 0; j < so.k; ++j) so.q[j] = o.q[j];
+        so.mat = o.dense;
+        pg.sops.push_back(so);
+      }
+    } else {
+      SchedParams p = sp;
+      p.nbits = nbits;
+      p.R = maxk > 4 ? 5 : 4;
+      std::string err;
+      if (plan_passes(p, fused, pg.plans, err) < 0) {
+        set_error(E_STATE, "scheduler: %s", err.c_str());
+        return false;
+      }
+      pack_pass_matrices(pg.plans, pool.data(), packed);
+      src = packed.data();
+      nsrc = packed.size();
+      pg.tmaps.resize(pg.plans.size());
+      char emsg[256];
+      for (size_t i = 0; i < pg.plans.size(); ++i)
+        if (encode_pass_tmap(&pg.tmaps[i], d_state, nbits, pg.plans[i].desc, emsg, sizeof(emsg)) != 0) {
+          set_error(E_CUDA, "%s", emsg);
           return false;
+        }
+    }
+    pg.pool_elems = nsrc;
+    if (own) {
+      if (nsrc) {
+        if (!cuda_ok(cudaMalloc(&pg.d_mats, nsrc * sizeof(double2)), "cudaMalloc program matrices")) return false;
         pg.owns = true;
-        if (!cuda_ok(cudaMemcpy(pg.d_mats, pool.data(), pool.size() * sizeof(double2), cudaMemcpyHostToDevice),
+        if (!cuda_ok(cudaMemcpy(pg.d_mats, src, nsrc * sizeof(double2), cudaMemcpyHostToDevice),
                      "H2D program matrices"))
           return false;
       }
     } else {
-      if (!upload_pool()) return false;
+      if (!upload_pool(reinterpret_cast<const double2*>(src), nsrc)) return false;
       pg.d_mats = d_pool;
     }
-    int maxk = 1;
-    for (auto& o : ops) maxk = std::max<int>(maxk, o.k);
-    pg.tiled = !eager && nbits >= 7;
-    if (!pg.tiled) {
-      for (size_t i = 0; i < ops.size(); ++i) {
-        SimpleOp so{};
-        so.k = ops[i].k;
-        for (int j = 0; j < so.k; ++j) so.q[j] = ops[i].q[j];
-        so.mat = dense_off[i];
-        pg.sops.push_back(so);
-      }
-      return true;
-    }
-    SchedParams p = sp;
-    p.nbits = nbits;
-    p.R = maxk > 4 ? 5 : 4;
-    std::string err;
-    if (plan_passes(p, ops, pg.plans, err) < 0) {
-      set_error(E_STATE, "scheduler: %s", err.c_str());
-      return false;
-    }
-    pg.tmaps.resize(pg.plans.size());
-    char emsg[256];
-    for (size_t i = 0; i < pg.plans.size(); ++i)
-      if (encode_pass_tmap(&pg.tmaps[i], d_state, nbits, pg.plans[i].desc, emsg, sizeof(emsg)) != 0) {
-        set_error(E_CUDA, "%s", emsg);
-        return false;
-      }
     return true;
   }
 
@@ -460,7 +468,6 @@ struct Engine {
 
   void clear_queue() {
     ops.clear();
-    dense_off.clear();
     pool.clear();
   }
 
@@ -468,7 +475,6 @@ struct Engine {
     if (ops.empty() || recording) return true;
     if (!select()) return false;
     ++st_flushes;
-    st_h2d += (double)pool.size() * sizeof(double2);
     Program pg;
     const bool ok = build_program(pg, false) && run_program(pg);
     clear_queue();
@@ -1010,9 +1016,7 @@ int iq_statevector_set_amplitudes(void* sv, const double* real_in, const double*
   Engine* e = as_engine(sv, 0);
   if (!e || !real_in || !imag_in) return -1;
   if (!e->select()) return -1;
-  e->ops.clear();
-  e->dense_off.clear();
-  e->pool.clear();
+  e->clear_queue();
   if (!e->ensure_stage()) return -1;
   const uint64_t per = kStageBytes / 16;
   for (uint64_t off = 0; off < e->dim; off += per) {
@@ -1053,7 +1057,9 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; }
   else if (!strcmp(key, "nbuf")) { if (iv < 1 || iv > 4) return -1; e->tl.nbuf = iv; }
   else if (!strcmp(key, "ctas_per_sm")) { if (iv < 1 || iv > 4) return -1; e->tl.ctas_per_sm = iv; }
+  else if (!strcmp(key, "consumers")) { if (iv != 128 && iv != 256) return -1; e->tl.consumers = iv; }
   else if (!strcmp(key, "eager")) e->eager = iv ? 1 : 0;
+  else if (!strcmp(key, "fuse")) e->fuse = iv ? 1 : 0;
   else if (!strcmp(key, "flush_ops")) { if (iv < 1) return -1; e->flush_ops = iv; }
   else if (!strcmp(key, "profile")) e->profile = iv ? 1 : 0;
   else { set_error(E_ARG, "unknown option '%s'", key); return -1; }
@@ -1069,7 +1075,9 @@ double iq_handle_get_option(void* h, const char* key) {
   if (!strcmp(key, "budget")) return e->sp.budget;
   if (!strcmp(key, "nbuf")) return e->tl.nbuf;
   if (!strcmp(key, "ctas_per_sm")) return e->tl.ctas_per_sm;
+  if (!strcmp(key, "consumers")) return e->tl.consumers;
   if (!strcmp(key, "eager")) return e->eager;
+  if (!strcmp(key, "fuse")) return e->fuse;
   if (!strcmp(key, "flush_ops")) return e->flush_ops;
   if (!strcmp(key, "profile")) return e->profile;
   return kNaN;

@@ -14,9 +14,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <array>
 #include <set>
 
 namespace iqb {
+
+// complex elements of an operation's matrix data (dense 4^k, monomial 2^k phases)
+int op_mat_elems(const SchedOp& op) { return op.mono ? (1 << op.k) : (1 << (2 * op.k)); }
 
 double op_cost(const SchedOp& op) {
   if (op.mono) return op.unit ? 0.25 : 4.0;
@@ -57,6 +61,7 @@ namespace {
 struct Stage {
   int S[kMaxK];
   int nS = 0;
+  uint64_t lanereq = 0;            // bits that 1q lane operations of this stage act on
   bool dk = false;                 // holds one dense k>=3 block; closed
   std::vector<int> ops;
 };
@@ -77,23 +82,18 @@ struct PassBuilder {
     for (int i = 0; i < s.nS; ++i) n += s.S[i] < c;
     return n;
   }
-  // lowest 3 bits of [0, c) not in S
-  bool isLane(const Stage& s, int b) const {
-    if (b >= c || inS(s, b)) return false;
-    int seen = 0;
-    for (int x = 0; x < c && seen < kLaneBits; ++x) {
-      if (inS(s, x)) continue;
-      if (x == b) return true;
-      ++seen;
-    }
-    return false;
-  }
-  // try to add operation bits to stage s (k <= 2); returns false if it does not fit
+  // Register slots take at most c - 3 of the chunk bits [0, c), so three lane
+  // bits always remain inside the chunk; lane operations name up to 3 of them.
   bool tryAdd(Stage& s, const SchedOp& op) const {
     if (s.dk) return false;
     if (op.k == 1) {
       const int b = op.q[0];
-      if (inS(s, b) || isLane(s, b)) return true;
+      const uint64_t bm = 1ULL << b;
+      if (inS(s, b) || (s.lanereq & bm)) return true;
+      if (b < c && __builtin_popcountll(s.lanereq) < kLaneBits) {
+        s.lanereq |= bm;
+        return true;
+      }
       if (s.nS >= p.R) return false;
       if (b < c && lowcount(s) + 1 > c - kLaneBits) return false;
       s.S[s.nS++] = b;
@@ -104,10 +104,12 @@ struct PassBuilder {
       if (!inS(s, op.q[i])) { need[nn++] = op.q[i]; lowadd += op.q[i] < c; }
     if (s.nS + nn > p.R) return false;
     if (lowcount(s) + lowadd > c - kLaneBits) return false;
-    for (int i = 0; i < nn; ++i) s.S[s.nS++] = need[i];
+    for (int i = 0; i < nn; ++i) {
+      s.S[s.nS++] = need[i];
+      s.lanereq &= ~(1ULL << need[i]);   // earlier lane ops on this bit become slot ops
+    }
     return true;
   }
-  // place op i; returns false if the pass cannot take it
   bool place(int idx, const SchedOp& op) {
     if (op.k >= 3) {
       if (op.k > p.R) return false;
@@ -135,6 +137,46 @@ struct PassBuilder {
     return true;
   }
 };
+
+// Rank over GF(2) of the low three bits of swz(1 << j) for the lane bits: the
+// eight lanes of an octet hit distinct shared-memory bank groups iff it is 3.
+int lane_rank(const int* l) {
+  uint32_t v[3];
+  for (int i = 0; i < 3; ++i) v[i] = swz(1u << l[i]) & 7u;
+  int r = 0;
+  for (int bit = 0; bit < 3; ++bit) {
+    int piv = -1;
+    for (int i = r; i < 3; ++i)
+      if (v[i] & (1u << bit)) { piv = i; break; }
+    if (piv < 0) continue;
+    std::swap(v[r], v[piv]);
+    for (int i = 0; i < 3; ++i)
+      if (i != r && (v[i] & (1u << bit))) v[i] ^= v[r];
+    ++r;
+  }
+  return r;
+}
+
+// Choose the 3 lane bits (tile-local) among `cand`, containing `req`, with the
+// best bank-group rank (ties: lowest bits).
+bool choose_lanes(const std::vector<int>& cand, uint32_t req, int out[3]) {
+  int best = -1;
+  const int n = (int)cand.size();
+  for (int a = 0; a < n; ++a)
+    for (int b = a + 1; b < n; ++b)
+      for (int d = b + 1; d < n; ++d) {
+        const int l[3] = {cand[a], cand[b], cand[d]};
+        const uint32_t m = (1u << l[0]) | (1u << l[1]) | (1u << l[2]);
+        if ((m & req) != req) continue;
+        const int r = lane_rank(l);
+        if (r > best) {
+          best = r;
+          out[0] = l[0]; out[1] = l[1]; out[2] = l[2];
+          if (r == 3) return true;
+        }
+      }
+  return best >= 0;
+}
 
 inline uint64_t opmask(const SchedOp& op) {
   uint64_t m = 0;
@@ -201,6 +243,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     PassBuilder pb(p, c);
     std::vector<int> taken;
     double cost = 0.0;
+    int mat_elems = 0;
     for (;;) {
       bool progress = true;
       while (progress) {
@@ -210,9 +253,11 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
           const SchedOp& o = ops[i];
           const double oc = op_cost(o);
           if ((opmask(o) & ~local) == 0 && (int)taken.size() < kMaxPassOps &&
-              (taken.empty() || cost + oc <= p.budget) && pb.place(i, o)) {
+              mat_elems + op_mat_elems(o) <= kSmemMatElems && (taken.empty() || cost + oc <= p.budget) &&
+              pb.place(i, o)) {
             taken.push_back(i);
             cost += oc;
+            mat_elems += op_mat_elems(o);
             it = ready.erase(it);
             retire(i);
             progress = true;
@@ -274,13 +319,28 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         slot_of[j] = nS++;
         used[j] = true;
       }
-      for (int j = M - 1; nS < p.R && j >= 0; --j)
-        if (!used[j]) { sd.S[nS] = (uint8_t)j; slot_of[j] = nS++; used[j] = true; }
-      int nl = 0;
+      // lanes: chunk bits for stages with lane operations, any tile bit for the
+      // others; padding slots come from the highest bits left over
+      uint32_t req = 0;
+      for (int b = 0; b < c; ++b)
+        if (s.lanereq & (1ULL << b)) req |= 1u << pos[b];
+      std::vector<int> cand;
+      const int lim = s.lanereq ? c : M;
+      for (int j = 0; j < lim; ++j)
+        if (!used[j]) cand.push_back(j);
+      // keep R - nS bits for padding out of the candidates' reach when possible
+      int lanes[3];
+      if (!choose_lanes(cand, req, lanes)) { err = "internal: no lane bits for a stage"; return -1; }
       int lane_of[kMaxTileBits];
       for (int j = 0; j < kMaxTileBits; ++j) lane_of[j] = -1;
-      for (int j = 0; j < M && nl < kLaneBits; ++j)
-        if (!used[j]) { sd.lane[nl] = (uint8_t)j; lane_of[j] = nl++; used[j] = true; }
+      for (int l = 0; l < kLaneBits; ++l) {
+        sd.lane[l] = (uint8_t)lanes[l];
+        lane_of[lanes[l]] = l;
+        used[lanes[l]] = true;
+      }
+      for (int j = M - 1; nS < p.R && j >= 0; --j)
+        if (!used[j]) { sd.S[nS] = (uint8_t)j; slot_of[j] = nS++; used[j] = true; }
+      if (nS < p.R) { err = "internal: not enough tile bits for the register slots"; return -1; }
       sd.nt = 0;
       for (int j = 0; j < M; ++j)
         if (!used[j]) sd.tb[sd.nt++] = (uint8_t)j;
@@ -317,6 +377,213 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     out.push_back(plan);
   }
   return (int)out.size();
+}
+
+namespace {
+
+using M4 = std::array<cplx64, 16>;
+
+inline cplx64 cm(cplx64 a, cplx64 b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline cplx64 ca(cplx64 a, cplx64 b) { return {a.re + b.re, a.im + b.im}; }
+
+M4 mul4(const M4& A, const M4& B) {
+  M4 C;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      cplx64 acc{0.0, 0.0};
+      for (int k = 0; k < 4; ++k) acc = ca(acc, cm(A[r * 4 + k], B[k * 4 + c]));
+      C[r * 4 + c] = acc;
+    }
+  return C;
+}
+
+// 2x2 U acting on local bit `bit` of a two-bit index (bit 0 = list[0])
+M4 lift1(const cplx64* U, int bit) {
+  M4 L;
+  for (auto& x : L) x = {0.0, 0.0};
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      const int ob = bit ^ 1;
+      if (((r >> ob) & 1) != ((c >> ob) & 1)) continue;
+      L[r * 4 + c] = U[((r >> bit) & 1) * 2 + ((c >> bit) & 1)];
+    }
+  return L;
+}
+
+// 4x4 U on list (u0, u1) re-expressed on list (l0, l1) = (u1, u0)
+M4 swap_bits(const cplx64* U) {
+  M4 L;
+  auto sw = [](int i) { return ((i & 1) << 1) | ((i >> 1) & 1); };
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) L[sw(r) * 4 + sw(c)] = U[r * 4 + c];
+  return L;
+}
+
+struct Block {
+  int k = 0;
+  int q[2] = {-1, -1};
+  M4 m;                 // dense (1q blocks use the top-left 2x2 in m[0], m[1], m[4], m[5])
+  bool dead = false;
+  int src = -1;         // index of the original op when the block is that op unchanged
+  bool changed = false;
+};
+
+}  // namespace
+
+std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool) {
+  const int nb = 64;
+  std::vector<Block> blocks;
+  std::vector<int> open(nb, -1), last(nb, -1);
+  std::vector<int> passthrough;   // ops of width >= 3 keep their place as blocks with k = 0
+  auto mat2 = [&](const SchedOp& o) {
+    M4 m;
+    const cplx64* U = pool.data() + o.dense;
+    m[0] = U[0]; m[1] = U[1]; m[4] = U[2]; m[5] = U[3];
+    return m;
+  };
+  for (size_t i = 0; i < ops.size(); ++i) {
+    const SchedOp& o = ops[i];
+    if (o.k >= 3) {
+      for (int j = 0; j < o.k; ++j) { open[o.q[j]] = -1; last[o.q[j]] = (int)blocks.size(); }
+      Block b;
+      b.k = 0;
+      b.src = (int)i;
+      blocks.push_back(b);
+      continue;
+    }
+    if (o.k == 1) {
+      const int a = o.q[0];
+      const int B = open[a];
+      if (B >= 0 && last[a] == B) {
+        Block& bl = blocks[B];
+        const cplx64 U[4] = {pool[o.dense], pool[o.dense + 1], pool[o.dense + 2], pool[o.dense + 3]};
+        if (bl.k == 1) {
+          M4 u1 = mat2(o);
+          M4 r;
+          for (auto& x : r) x = {0.0, 0.0};
+          for (int rr = 0; rr < 2; ++rr)
+            for (int cc = 0; cc < 2; ++cc)
+              for (int kk = 0; kk < 2; ++kk)
+                r[rr * 4 + cc] = ca(r[rr * 4 + cc], cm(u1[rr * 4 + kk], bl.m[kk * 4 + cc]));
+          bl.m = r;
+        } else {
+          bl.m = mul4(lift1(U, bl.q[0] == a ? 0 : 1), bl.m);
+        }
+        bl.changed = true;
+        bl.src = -1;
+        continue;
+      }
+      Block b;
+      b.k = 1;
+      b.q[0] = a;
+      b.m = mat2(o);
+      b.src = (int)i;
+      open[a] = last[a] = (int)blocks.size();
+      blocks.push_back(b);
+      continue;
+    }
+    // two-qubit op on list (a, b) (bit 0 = a)
+    const int a = o.q[0], bq = o.q[1];
+    const int Ba = open[a], Bb = open[bq];
+    const cplx64* U = pool.data() + o.dense;
+    M4 Um;
+    for (int j = 0; j < 16; ++j) Um[j] = U[j];
+    if (Ba >= 0 && Ba == Bb && last[a] == Ba && last[bq] == Ba && blocks[Ba].k == 2) {
+      Block& bl = blocks[Ba];
+      bl.m = mul4(bl.q[0] == a ? Um : swap_bits(Um.data()), bl.m);
+      bl.changed = true;
+      bl.src = -1;
+      continue;
+    }
+    const bool okA = Ba < 0 || (blocks[Ba].k == 1 && last[a] == Ba);
+    const bool okB = Bb < 0 || (blocks[Bb].k == 1 && last[bq] == Bb);
+    const int posc = std::max(Ba, Bb);
+    // the fused block goes to position posc: nothing after it may touch a or b
+    const bool okPos = posc >= 0 && last[a] <= posc && last[bq] <= posc;
+    Block nbk;
+    nbk.k = 2;
+    nbk.q[0] = a;
+    nbk.q[1] = bq;
+    if (okA && okB && okPos) {
+      // the fused block sits at the later of the two one-qubit blocks; moving the
+      // earlier one there is valid because it is the last block on its qubit
+      M4 pre;
+      for (auto& x : pre) x = {0.0, 0.0};
+      for (int j = 0; j < 4; ++j) pre[j * 5] = {1.0, 0.0};
+      if (Ba >= 0) {
+        const cplx64 ua[4] = {blocks[Ba].m[0], blocks[Ba].m[1], blocks[Ba].m[4], blocks[Ba].m[5]};
+        pre = mul4(lift1(ua, 0), pre);
+      }
+      if (Bb >= 0) {
+        const cplx64 ub[4] = {blocks[Bb].m[0], blocks[Bb].m[1], blocks[Bb].m[4], blocks[Bb].m[5]};
+        pre = mul4(lift1(ub, 1), pre);
+      }
+      nbk.m = mul4(Um, pre);
+      nbk.changed = true;
+      const int pos = std::max(Ba, Bb);
+      const int other = std::min(Ba, Bb);
+      if (other >= 0 && other != pos) blocks[other].dead = true;
+      blocks[pos] = nbk;
+      open[a] = open[bq] = last[a] = last[bq] = pos;
+      continue;
+    }
+    nbk.m = Um;
+    nbk.src = (int)i;
+    open[a] = open[bq] = last[a] = last[bq] = (int)blocks.size();
+    blocks.push_back(nbk);
+  }
+  std::vector<SchedOp> out;
+  out.reserve(blocks.size());
+  for (const Block& b : blocks) {
+    if (b.dead) continue;
+    if (b.src >= 0 && !b.changed) {
+      out.push_back(ops[b.src]);
+      continue;
+    }
+    SchedOp o{};
+    o.k = (uint8_t)b.k;
+    const int d = 1 << b.k;
+    o.dense = (uint32_t)pool.size();
+    double flat[32];
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c) {
+        const cplx64 v = b.m[r * 4 + c];
+        pool.push_back(v);
+        flat[2 * (r * d + c)] = v.re;
+        flat[2 * (r * d + c) + 1] = v.im;
+      }
+    for (int j = 0; j < b.k; ++j) o.q[j] = (uint8_t)b.q[j];
+    o.mat = o.dense;
+    double ph[8];
+    uint8_t perm = 0, unit = 0;
+    if (classify_monomial(flat, b.k, &perm, ph, &unit)) {
+      o.mono = 1;
+      o.perm = perm;
+      o.unit = unit;
+      o.mat = (uint32_t)pool.size();
+      for (int j = 0; j < d; ++j) pool.push_back({ph[2 * j], ph[2 * j + 1]});
+    }
+    out.push_back(o);
+  }
+  return out;
+}
+
+void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::vector<cplx64>& packed) {
+  packed.clear();
+  for (auto& pl : plans) {
+    PassDesc& d = pl.desc;
+    const uint32_t base = (uint32_t)packed.size();
+    for (uint32_t i = 0; i < d.nops; ++i) {
+      OpDesc& od = d.ops[i];
+      const bool mono = od.kind == OP_M1R || od.kind == OP_M1L || od.kind == OP_M2R;
+      const uint32_t n = mono ? (1u << od.k) : (1u << (2 * od.k));
+      const uint32_t rel = (uint32_t)packed.size() - base;
+      packed.insert(packed.end(), pool + od.mat, pool + od.mat + n);
+      od.mat = rel;
+    }
+    d.mat_base = base;
+    d.mat_elems = (uint32_t)packed.size() - base;
+  }
 }
 
 }  // namespace iqb

@@ -24,7 +24,8 @@ struct Emu {
   cd* state;
   std::string err;
 
-  cd mat(uint32_t off, int i) const { return pool[off + i]; }
+  uint32_t blk = 0;   // current pass's matrix block
+  cd mat(uint32_t off, int i) const { return pool[blk + off + i]; }
 
   bool copy_tile(const PassDesc& P, uint64_t t, std::vector<cd>& tile, bool load, std::vector<uint8_t>& seen) {
     uint64_t gd[5], gs[4];
@@ -53,7 +54,9 @@ struct Emu {
                 if (g % 8) { err = "misaligned element"; return false; }
                 const uint64_t gi = g / 8;
                 if (gi >= (2ull << nbits)) { err = "global address out of range"; return false; }
-                const uint64_t si = (uint64_t)j * box_elems * 2 + lin;
+                // TMA 128-byte swizzle: 16-byte unit u of the tile lands in slot swz(u)
+                const uint64_t lin_d = (uint64_t)j * box_elems * 2 + lin;
+                const uint64_t si = 2 * (uint64_t)swz((uint32_t)(lin_d / 2)) + (lin_d & 1);
                 if (si >= tile.size() * 2) { err = "shared address out of range"; return false; }
                 if (load) {
                   td[si] = sd[gi];
@@ -86,7 +89,7 @@ struct Emu {
       uint32_t base[8];
       for (int L = 0; L < 8; ++L) {
         base[L] = ub | ((L & 1u) << sd.lane[0]) | (((L >> 1) & 1u) << sd.lane[1]) | (((L >> 2) & 1u) << sd.lane[2]);
-        for (int v = 0; v < NV; ++v) a[L][v] = tile[base[L] | voff(v)];
+        for (int v = 0; v < NV; ++v) a[L][v] = tile[swz(base[L] | voff(v))];
       }
       bool stored = false;
       for (int o = sd.op0; o < sd.op1; ++o) {
@@ -166,7 +169,7 @@ struct Emu {
                 for (int r = 0; r < D; ++r) {
                   cd acc = 0.0;
                   for (int cc = 0; cc < D; ++cc) acc += mat(od.mat, r * D + cc) * a[L][g + cc];
-                  tile[base[L] | voff(g + r)] = acc;
+                  tile[swz(base[L] | voff(g + r))] = acc;
                 }
             stored = true;
             break;
@@ -178,7 +181,7 @@ struct Emu {
       }
       if (!stored)
         for (int L = 0; L < 8; ++L)
-          for (int v = 0; v < NV; ++v) tile[base[L] | voff(v)] = a[L][v];
+          for (int v = 0; v < NV; ++v) tile[swz(base[L] | voff(v))] = a[L][v];
     }
     return true;
   }
@@ -186,9 +189,9 @@ struct Emu {
 
 }  // namespace
 
-extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double budget, int nops, const int* ks,
-                         const int* qs, const double* mats, const long long* mat_off, double* state_il,
-                         int* npasses, int* ops_per_pass, char* errbuf, int errlen) {
+extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double budget, int fuse, int nops,
+                         const int* ks, const int* qs, const double* mats, const long long* mat_off,
+                         double* state_il, int* npasses, int* ops_per_pass, char* errbuf, int errlen) {
   Emu e;
   e.nbits = nbits;
   e.state = reinterpret_cast<cd*>(state_il);
@@ -200,6 +203,7 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
     const int d = 1 << ks[i];
     const double* m = mats + 2 * mat_off[i];
     o.mat = (uint32_t)e.pool.size();
+    o.dense = o.mat;
     for (int j = 0; j < d * d; ++j) e.pool.emplace_back(m[2 * j], m[2 * j + 1]);
     double ph[8];
     uint8_t perm = 0, unit = 0;
@@ -211,6 +215,12 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
       for (int j = 0; j < d; ++j) e.pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
     }
     ops.push_back(o);
+  }
+  if (fuse) {
+    std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(e.pool.data()),
+                           reinterpret_cast<const cplx64*>(e.pool.data()) + e.pool.size());
+    ops = fuse_two_qubit_blocks(ops, cp);
+    e.pool.assign(reinterpret_cast<const cd*>(cp.data()), reinterpret_cast<const cd*>(cp.data()) + cp.size());
   }
   SchedParams p{};
   p.nbits = nbits;
@@ -226,8 +236,16 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
     return -1;
   }
   *npasses = (int)plans.size();
+  std::vector<cplx64> packed;
+  pack_pass_matrices(plans, reinterpret_cast<const cplx64*>(e.pool.data()), packed);
+  e.pool.assign(reinterpret_cast<const cd*>(packed.data()), reinterpret_cast<const cd*>(packed.data()) + packed.size());
   for (size_t pi = 0; pi < plans.size(); ++pi) {
     const PassDesc& P = plans[pi].desc;
+    e.blk = P.mat_base;
+    if (P.mat_elems > (uint32_t)kSmemMatElems) {
+      snprintf(errbuf, errlen, "pass %zu: matrix block exceeds shared memory", pi);
+      return -1;
+    }
     if (ops_per_pass) ops_per_pass[pi] = plans[pi].nsrc;
     std::vector<cd> tile((size_t)1 << P.M);
     std::vector<uint8_t> seen((size_t)1 << nbits, 0);

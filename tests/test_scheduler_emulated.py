@@ -75,7 +75,7 @@ def apply_lsb_numpy(state, n, qs, U):
     return np.transpose(out, np.argsort(list(qs) + rest)).reshape(-1, order="F")
 
 
-def run_emu(emu, n, lsb_ops, state, M=12, c=5, R=4, max_stages=8, budget=80.0):
+def run_emu(emu, n, lsb_ops, state, M=12, c=5, R=4, max_stages=8, budget=80.0, fuse=1):
     nops = len(lsb_ops)
     ks = np.array([len(q) for q, _ in lsb_ops], dtype=np.int32)
     qs = np.full((nops, 5), -1, dtype=np.int32)
@@ -93,7 +93,7 @@ def run_emu(emu, n, lsb_ops, state, M=12, c=5, R=4, max_stages=8, budget=80.0):
     npasses = ctypes.c_int(0)
     per = np.zeros(max(nops, 1), dtype=np.int32)
     err = ctypes.create_string_buffer(512)
-    rc = emu.emu_apply(n, M, c, R, max_stages, ctypes.c_double(budget), nops,
+    rc = emu.emu_apply(n, M, c, R, max_stages, ctypes.c_double(budget), fuse, nops,
                        ks.ctypes.data_as(ctypes.c_void_p), qs.ctypes.data_as(ctypes.c_void_p),
                        pool.ctypes.data_as(ctypes.c_void_p), offs.ctypes.data_as(ctypes.c_void_p),
                        st.ctypes.data_as(ctypes.c_void_p), ctypes.byref(npasses),
@@ -137,9 +137,11 @@ def test_emulated_passes_match_oracle(port, emu, n, M, c, R, stages, budget, see
     start = ref.copy()
     ref = oracle_apply(port, ref, n, ops)
     lsb = [to_lsb(*o) for o in ops]
-    got, npasses, per = run_emu(emu, n, lsb, start, M=M, c=c, R=R, max_stages=stages, budget=budget)
-    assert per.sum() == len(ops)
-    assert np.max(np.abs(got - ref)) < 1e-12
+    for fuse in (0, 1):
+        got, npasses, per = run_emu(emu, n, lsb, start, M=M, c=c, R=R, max_stages=stages, budget=budget, fuse=fuse)
+        assert per.sum() <= len(ops)
+        assert fuse or per.sum() == len(ops)
+        assert np.max(np.abs(got - ref)) < 1e-12
 
 
 def brickwall_ops(n, depth, seed):
