@@ -158,6 +158,25 @@ void  iq_program_free(void* prog);
  * returns up to max per-pass durations in ms (oldest first) and clears them. */
 int iq_handle_profile_read(void* h, double* ms_out, size_t max);
 
+/* <Z_q> for q = 0..num_qubits-1 of a complex128 amplitude array the caller
+ * holds in device memory (d_amps, 2^num_qubits elements), written to the
+ * caller's device array d_out (num_qubits doubles), launched on `stream`
+ * (a cudaStream_t; results are ready when the stream reaches them).  No
+ * counterpart in the reference.  It allocates no memory of any kind: it is for
+ * callers that cannot call cudaMalloc where they need the result -- a host
+ * whose device memory is already committed (a 33-qubit state fills 128 GiB) or
+ * code running inside another framework that owns the free device memory.  Its
+ * reduction scratch is a fixed array in the library (about 166 KB per GPU,
+ * held until the process exits), so num_qubits is limited to
+ * IQ_NOALLOC_MAX_QUBITS and larger sizes are rejected with an error.  The
+ * first call on each device looks up that array's device address once; make
+ * that first call before any stream capture.  All calls on one device share
+ * the array, so calls that overlap on the GPU (different streams, no ordering
+ * between them) race and must be avoided.  Returns 0, or -1 with iq_last_error
+ * set. */
+#define IQ_NOALLOC_MAX_QUBITS 34
+int iq_statevector_expval_z_all_noalloc(const void* d_amps, size_t num_qubits, double* d_out, void* stream);
+
 /* Density-matrix additions. */
 int iq_density_matrix_flush(void* dm);
 /* Kraus channel on two qubits: num_kraus 4x4 matrices, q0 = most significant

@@ -97,6 +97,7 @@ SIGNATURES = {
     "iq_handle_program_run": ([_v, _v], _i),
     "iq_program_info": ([_v, c_dp, _sz], _i),
     "iq_program_free": ([_v], None),
+    "iq_statevector_expval_z_all_noalloc": ([_v, _sz, _v, _v], _i),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),
     "iq_density_matrix_get_diagonal": ([_v, c_dp], None),

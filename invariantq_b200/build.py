@@ -25,7 +25,7 @@ INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", *ARCH]
-SOURCES = ["iq_kernels.cu", "iq_runtime.cu", "iq_sched.cpp"]
+SOURCES = ["iq_kernels.cu", "iq_runtime.cu", "iq_sched.cpp", "iq_noalloc.cu"]
 HEADERS = ["iq_kernels.h", "iq_plan.h"]
 
 

@@ -75,4 +75,7 @@ cudaError_t launch_block_search(const double2* s, int bbits, const uint64_t* blk
 // rho_A[r][c] = sum_env a[idx(r,env)] conj(a[idx(c,env)]), keep[] LSB-first (k <= 12)
 cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, int k, double2* out, cudaStream_t st);
 
+// Record an error for iq_last_error (defined in iq_runtime.cu).
+void record_error(int code, const char* msg);
+
 }  // namespace iqb

@@ -626,6 +626,8 @@ struct CpuCore {
 
 }  // namespace
 
+void iqb::record_error(int code, const char* msg) { set_error(code, "%s", msg); }
+
 extern "C" {
 
 // ============================================================ errors / info
