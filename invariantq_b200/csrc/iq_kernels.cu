@@ -1,19 +1,7 @@
-// iq_kernels.cu -- sm_100a kernels for the state-vector / density-matrix path.
-//
-// Hot kernel: tile_pass_kernel.  One launch = one pass over the complex128
-// array (16 B per amplitude read once, written once).  Per CTA one producer
-// warp moves 2^M-amplitude tiles between HBM and shared memory with TMA tensor
-// copies (cp.async.bulk.tensor, mbarrier completion), through an NBUF-deep ring
-// of tile buffers; the consumer warps apply the pass's register stages (see
-// iq_plan.h) to the resident tile.  This replaces the reference's per-gate
-// OpenMP sweeps (core/src/statevector.cpp:26-152) and its two-pass density-
-// matrix updates (core/src/density_matrix.cpp:18-163): a density matrix is the
-// same array with 2n index bits, U rho U^dagger is U on the row bits and
-// conj(U) on the column bits, and a Kraus channel is the 4x4 superoperator
-// sum_k K_k (x) conj(K_k) on the (row, column) bit pair.
-//
-// Every wait on an mbarrier is bounded; a wait that runs out sets a status word
-// the host reads, and the CTA finishes its loop without further copies.
+// iq_kernels.cu -- host launchers and the non-tile sm_100a kernels: tensor-map
+// encoding, the launcher of the tile pass (kernel in iq_tile.cuh, instantiated
+// in iq_tile_r4.cu / iq_tile_r5.cu), the one-operation global-memory kernel,
+// FP64 reductions, elementwise kernels, sampling and the partial trace.
 #include <cudaTypedefs.h>
 
 #include <cstdio>
@@ -36,603 +24,9 @@ __device__ __forceinline__ double2 cfma(double2 acc, double2 a, double2 b) {
   acc.y = fma(a.y, b.x, acc.y);
   return acc;
 }
-// operation matrices are read from the pass's block in shared memory
 __device__ __forceinline__ double2 ld_mat(const double2* m, int i) { return m[i]; }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done;
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
-                                            int c4, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
-      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
-                                             const void* src) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
-      " [%0, {%2, %3, %4, %5, %6}], [%1];" ::"l"(tm),
-      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
-      : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-// Wait limit of one mbarrier phase: 2 s of %globaltimer (a tile load or a
-// consumer stage takes microseconds).
-constexpr uint64_t kWaitLimitNs = 2000000000ull;
-
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait that ignores the abort flag: used to let copies already in
-// flight land before the CTA exits after an abort.
-__device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity) {
-  const uint64_t t0 = global_ns();
-  while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kWaitLimitNs) return;
-}
-
-// Bounded wait on an mbarrier phase.  Returns false (and raises the abort flag
-// plus the status word) when the limit runs out, or as soon as another thread
-// of the CTA has aborted.
-__device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                             int* status, int code) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_ns();
-  for (;;) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (*abort_flag) return false;
-    if (global_ns() - t0 > kWaitLimitNs) break;
-  }
-  *abort_flag = 1;
-  atomicCAS(status, 0, code);
-  return false;
-}
-
-// ------------------------------------------------------- register-slot ops
-//
-// Every operation reads the register array `s` and writes all of its outputs
-// to `d`.  With R = 4 the stage alternates between two arrays (ping-pong), so
-// results go straight to their final registers.  With R = 5 (32 amplitudes per
-// thread) there is room for one array only and the same code runs in place
-// (s and d alias); the INPLACE flag selects orders that stay correct then.
-
-template <int R, int S>
-__device__ __forceinline__ void d1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    if (v & (1 << S)) continue;
-    const double2 x = s[v], y = s[v | (1 << S)];
-    d[v] = cfma(cmul(u0, x), u1, y);
-    d[v | (1 << S)] = cfma(cmul(u2, x), u3, y);
-  }
-}
-
-template <int R, int S, bool SW, bool UNIT>
-__device__ __forceinline__ void m1r_t(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  double2 p0 = make_double2(1.0, 0.0), p1 = p0;
-  if (!UNIT) { p0 = ld_mat(m, 0); p1 = ld_mat(m, 1); }
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    if (v & (1 << S)) continue;
-    double2 x = s[v], y = s[v | (1 << S)];
-    if (SW) { const double2 t = x; x = y; y = t; }
-    if (!UNIT) { x = cmul(p0, x); y = cmul(p1, y); }
-    d[v] = x;
-    d[v | (1 << S)] = y;
-  }
-}
-
-template <int R, int S>
-__device__ __forceinline__ void m1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int perm,
-                                    bool unit) {
-  if (perm & 1) {
-    if (unit) m1r_t<R, S, true, true>(s, d, m);
-    else m1r_t<R, S, true, false>(s, d, m);
-  } else if (unit) {
-    m1r_t<R, S, false, true>(s, d, m);
-  } else {
-    m1r_t<R, S, false, false>(s, d, m);
-  }
-}
-
-// dense 4x4 on slots A (matrix bit 0) and B (matrix bit 1).  Row-outer when
-// writing a separate array (one matrix row live at a time), group-outer in place.
-template <int R, int A, int B, bool INPLACE>
-__device__ __forceinline__ void d2r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  if constexpr (INPLACE) {
-#pragma unroll
-    for (int v = 0; v < (1 << R); ++v) {
-      if (v & ((1 << A) | (1 << B))) continue;
-      const int idx[4] = {v, v | (1 << A), v | (1 << B), v | (1 << A) | (1 << B)};
-      const double2 x[4] = {s[idx[0]], s[idx[1]], s[idx[2]], s[idx[3]]};
-      double2 o[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        double2 acc = cmul(ld_mat(m, 4 * r + 0), x[0]);
-        acc = cfma(acc, ld_mat(m, 4 * r + 1), x[1]);
-        acc = cfma(acc, ld_mat(m, 4 * r + 2), x[2]);
-        acc = cfma(acc, ld_mat(m, 4 * r + 3), x[3]);
-        o[r] = acc;
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) d[idx[r]] = o[r];
-    }
-  } else {
-    // two rows per step: 16 independent accumulation chains per thread
-#pragma unroll
-    for (int r = 0; r < 4; r += 2) {
-      const double2 u0 = ld_mat(m, 4 * r + 0), u1 = ld_mat(m, 4 * r + 1), u2 = ld_mat(m, 4 * r + 2),
-                    u3 = ld_mat(m, 4 * r + 3);
-      const double2 w0 = ld_mat(m, 4 * r + 4), w1 = ld_mat(m, 4 * r + 5), w2 = ld_mat(m, 4 * r + 6),
-                    w3 = ld_mat(m, 4 * r + 7);
-      const int ro = ((r & 1) << A) | (((r >> 1) & 1) << B);
-      const int ro1 = (((r + 1) & 1) << A) | ((((r + 1) >> 1) & 1) << B);
-#pragma unroll
-      for (int v = 0; v < (1 << R); ++v) {
-        if (v & ((1 << A) | (1 << B))) continue;
-        const double2 x0 = s[v], x1 = s[v | (1 << A)], x2 = s[v | (1 << B)], x3 = s[v | (1 << A) | (1 << B)];
-        double2 acc = cmul(u0, x0), acc1 = cmul(w0, x0);
-        acc = cfma(acc, u1, x1);
-        acc1 = cfma(acc1, w1, x1);
-        acc = cfma(acc, u2, x2);
-        acc1 = cfma(acc1, w2, x2);
-        acc = cfma(acc, u3, x3);
-        acc1 = cfma(acc1, w3, x3);
-        d[v | ro] = acc;
-        d[v | ro1] = acc1;
-      }
-    }
-  }
-}
-
-// Monomial 4x4 on slots A (matrix bit 0) and B (matrix bit 1): output row r
-// takes input column (PERM >> 2r) & 3 times phase r (inputs read before writes).
-template <int R, int A, int B, int PERM, bool UNIT>
-__device__ __forceinline__ void m2r_t(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  double2 p[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) p[r] = UNIT ? make_double2(1.0, 0.0) : ld_mat(m, r);
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    if (v & ((1 << A) | (1 << B))) continue;
-    const int idx[4] = {v, v | (1 << A), v | (1 << B), v | (1 << A) | (1 << B)};
-    const double2 x[4] = {s[idx[0]], s[idx[1]], s[idx[2]], s[idx[3]]};
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const double2 y = x[(PERM >> (2 * r)) & 3];
-      d[idx[r]] = UNIT ? y : cmul(p[r], y);
-    }
-  }
-}
-
-__device__ __forceinline__ double2 sel4(int i, double2 x0, double2 x1, double2 x2, double2 x3) {
-  const double2 lo = (i & 1) ? x1 : x0;
-  const double2 hi = (i & 1) ? x3 : x2;
-  return (i & 2) ? hi : lo;
-}
-
-template <int R, int A, int B>
-__device__ __forceinline__ void m2r_generic(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
-                                            int perm, bool unit) {
-  const int c0 = perm & 3, c1 = (perm >> 2) & 3, c2 = (perm >> 4) & 3, c3 = (perm >> 6) & 3;
-  double2 p0 = make_double2(1.0, 0.0), p1 = p0, p2 = p0, p3 = p0;
-  if (!unit) { p0 = ld_mat(m, 0); p1 = ld_mat(m, 1); p2 = ld_mat(m, 2); p3 = ld_mat(m, 3); }
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    if (v & ((1 << A) | (1 << B))) continue;
-    const int i0 = v, i1 = v | (1 << A), i2 = v | (1 << B), i3 = v | (1 << A) | (1 << B);
-    const double2 x0 = s[i0], x1 = s[i1], x2 = s[i2], x3 = s[i3];
-    double2 o0 = sel4(c0, x0, x1, x2, x3), o1 = sel4(c1, x0, x1, x2, x3);
-    double2 o2 = sel4(c2, x0, x1, x2, x3), o3 = sel4(c3, x0, x1, x2, x3);
-    if (!unit) { o0 = cmul(p0, o0); o1 = cmul(p1, o1); o2 = cmul(p2, o2); o3 = cmul(p3, o3); }
-    d[i0] = o0;
-    d[i1] = o1;
-    d[i2] = o2;
-    d[i3] = o3;
-  }
-}
-
-constexpr int kPermId = 0xE4;     // [0, 1, 2, 3]: diagonal gates (CZ, CP, CRZ)
-constexpr int kPermCx1 = 0xB4;    // [0, 1, 3, 2]: X on bit 0 controlled by bit 1
-constexpr int kPermCx0 = 0x6C;    // [0, 3, 2, 1]: X on bit 1 controlled by bit 0
-constexpr int kPermSwap = 0xD8;   // [0, 2, 1, 3]
-
-template <int R, int A, int B>
-__device__ __forceinline__ void m2r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int perm,
-                                    bool unit) {
-  if (unit) {
-    switch (perm) {
-      case kPermId: m2r_t<R, A, B, kPermId, true>(s, d, m); return;
-      case kPermCx1: m2r_t<R, A, B, kPermCx1, true>(s, d, m); return;
-      case kPermCx0: m2r_t<R, A, B, kPermCx0, true>(s, d, m); return;
-      case kPermSwap: m2r_t<R, A, B, kPermSwap, true>(s, d, m); return;
-      default: break;
-    }
-  } else if (perm == kPermId) {
-    m2r_t<R, A, B, kPermId, false>(s, d, m);
-    return;
-  }
-  m2r_generic<R, A, B>(s, d, m, perm, unit);
-}
-
-// shared-memory slot offset of register v: XOR of the (swizzled) slot bits
-// set in v; v is a compile-time constant after unrolling, so this folds to a
-// few XORs of values computed once per stage
-template <int R>
-__device__ __forceinline__ uint32_t voff(int v, const uint32_t (&sb)[R]) {
-  uint32_t o = 0;
-#pragma unroll
-  for (int i = 0; i < R; ++i)
-    if ((v >> i) & 1) o ^= sb[i];
-  return o;
-}
-
-// dense 2^K block on slots 0..K-1, written straight to the tile (ends the stage);
-// rows are a runtime loop so only one row of the matrix is live at a time
-template <int R, int K>
-__device__ __forceinline__ void dkr_store(const double2 (&a)[1 << R], const double2* m, double2* tile,
-                                          const uint32_t (&sb)[R], uint32_t base) {
-  constexpr int D = 1 << K;
-#pragma unroll
-  for (int g = 0; g < (1 << R); g += D) {
-    const uint32_t goff = base ^ voff<R>(g, sb);
-#pragma unroll 1
-    for (int r = 0; r < D; ++r) {
-      double2 acc = cmul(ld_mat(m, r * D), a[g]);
-#pragma unroll
-      for (int c = 1; c < D; ++c) acc = cfma(acc, ld_mat(m, r * D + c), a[g + c]);
-      uint32_t roff = 0;
-#pragma unroll
-      for (int i = 0; i < K; ++i)
-        if ((r >> i) & 1) roff ^= sb[i];
-      tile[goff ^ roff] = acc;
-    }
-  }
-}
-
-// lane-bit 1q ops: partner amplitude lives in lane ^ (1 << lb) of the octet
-__device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
-  return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
-}
-
-template <int R>
-__device__ __forceinline__ void d1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
-                                    int lane8, unsigned omask) {
-  const int my = (lane8 >> lb) & 1;
-  const double2 cs = my ? ld_mat(m, 3) : ld_mat(m, 0);
-  const double2 co = my ? ld_mat(m, 2) : ld_mat(m, 1);
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    const double2 x = s[v];
-    const double2 p = shfl_xor2(x, 1 << lb, omask);
-    d[v] = cfma(cmul(cs, x), co, p);
-  }
-}
-
-template <int R>
-__device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
-                                    int lane8, unsigned omask, int perm, bool unit) {
-  const int my = (lane8 >> lb) & 1;
-  const double2 ph = unit ? make_double2(1.0, 0.0) : (my ? ld_mat(m, 1) : ld_mat(m, 0));
-  const bool sw = perm & 1;
-#pragma unroll
-  for (int v = 0; v < (1 << R); ++v) {
-    double2 x = s[v];
-    if (sw) x = shfl_xor2(x, 1 << lb, omask);
-    d[v] = unit ? x : cmul(ph, x);
-  }
-}
-
-// ------------------------------------------------------- runtime dispatch
-
-template <int R, int S = 0>
-__device__ __forceinline__ void disp_d1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  if constexpr (S < R) {
-    if (sl == S) d1r<R, S>(s, d, m);
-    else disp_d1r<R, S + 1>(sl, s, d, m);
-  }
-}
-template <int R, int S = 0>
-__device__ __forceinline__ void disp_m1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
-                                         int perm, bool unit) {
-  if constexpr (S < R) {
-    if (sl == S) m1r<R, S>(s, d, m, perm, unit);
-    else disp_m1r<R, S + 1>(sl, s, d, m, perm, unit);
-  }
-}
-template <int R, bool IP, int A, int B = 0>
-__device__ __forceinline__ void disp_d2r_b(int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R],
-                                           const double2* m) {
-  if constexpr (B < R) {
-    if constexpr (A != B) {
-      if (sb == B) { d2r<R, A, B, IP>(s, d, m); return; }
-    }
-    disp_d2r_b<R, IP, A, B + 1>(sb, s, d, m);
-  }
-}
-template <int R, bool IP, int A = 0>
-__device__ __forceinline__ void disp_d2r(int sa, int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R],
-                                         const double2* m) {
-  if constexpr (A < R) {
-    if (sa == A) disp_d2r_b<R, IP, A>(sb, s, d, m);
-    else disp_d2r<R, IP, A + 1>(sa, sb, s, d, m);
-  }
-}
-template <int R, int A, int B = 0>
-__device__ __forceinline__ void disp_m2r_b(int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
-                                           int perm, bool unit) {
-  if constexpr (B < R) {
-    if constexpr (A != B) {
-      if (sb == B) { m2r<R, A, B>(s, d, m, perm, unit); return; }
-    }
-    disp_m2r_b<R, A, B + 1>(sb, s, d, m, perm, unit);
-  }
-}
-template <int R, int A = 0>
-__device__ __forceinline__ void disp_m2r(int sa, int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R],
-                                         const double2* m, int perm, bool unit) {
-  if constexpr (A < R) {
-    if (sa == A) disp_m2r_b<R, A>(sb, s, d, m, perm, unit);
-    else disp_m2r<R, A + 1>(sa, sb, s, d, m, perm, unit);
-  }
-}
-template <int R, int K = 3>
-__device__ __forceinline__ void disp_dkr(int k, const double2 (&a)[1 << R], const double2* m, double2* tile,
-                                         const uint32_t (&sb)[R], uint32_t base) {
-  if constexpr (K <= R) {
-    if (k == K) dkr_store<R, K>(a, m, tile, sb, base);
-    else disp_dkr<R, K + 1>(k, a, m, tile, sb, base);
-  }
-}
-
-// Apply one operation from s to d; returns true when it wrote the tile itself.
-template <int R, bool IP>
-__device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 << R], double2 (&d)[1 << R],
-                                         const double2* mats, int lane8, unsigned omask, double2* tile,
-                                         const uint32_t (&sb)[R], uint32_t base) {
-  const double2* m = mats + od.mat;
-  const bool unit = od.flags & OPF_UNIT_PHASE;
-  switch (od.kind) {
-    case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
-    case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
-    case OP_D2R: disp_d2r<R, IP>(od.a, od.b, s, d, m); break;
-    case OP_M1R: disp_m1r<R>(od.a, s, d, m, od.perm, unit); break;
-    case OP_M1L: m1l<R>(s, d, m, od.a, lane8, omask, od.perm, unit); break;
-    case OP_M2R: disp_m2r<R>(od.a, od.b, s, d, m, od.perm, unit); break;
-    case OP_DKR: disp_dkr<R>(od.k, s, m, tile, sb, base); return true;
-    default: break;
-  }
-  return false;
-}
-
-// One stage over the resident tile (consumer threads only).  Tile amplitude j
-// lives in shared-memory slot swz(j); every offset below is kept swizzled.
-template <int R>
-__device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int s, const double2* mats,
-                                          int ctid, int ncons) {
-  constexpr int NV = 1 << R;
-  const StageDesc& sd = P.st[s];
-  const int lane8 = ctid & 7;
-  const unsigned omask = 0xFFu << (ctid & 24);
-  const uint32_t laneoff = ((uint32_t)(lane8 & 1) << sd.lane[0]) | ((uint32_t)((lane8 >> 1) & 1) << sd.lane[1]) |
-                           ((uint32_t)((lane8 >> 2) & 1) << sd.lane[2]);
-  uint32_t sb[R];
-#pragma unroll
-  for (int i = 0; i < R; ++i) sb[i] = swz(1u << sd.S[i]);
-  const int nsub = 1 << sd.nt;
-  const int op0 = sd.op0, op1 = sd.op1;
-  for (int u = ctid >> 3; u < nsub; u += ncons >> 3) {
-    uint32_t base = laneoff;
-    for (int i = 0; i < sd.nt; ++i) base |= (uint32_t)((u >> i) & 1) << sd.tb[i];
-    base = swz(base);
-    double2 a[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) a[v] = tile[base ^ voff<R>(v, sb)];
-    bool stored = false;
-    if constexpr (R == 4) {
-      double2 b[NV];
-      int o = op0;
-      for (; o + 1 < op1; o += 2) {
-        stored |= apply_op<R, false>(P.ops[o], a, b, mats, lane8, omask, tile, sb, base);
-        stored |= apply_op<R, false>(P.ops[o + 1], b, a, mats, lane8, omask, tile, sb, base);
-      }
-      if (o < op1) {
-        stored |= apply_op<R, false>(P.ops[o], a, b, mats, lane8, omask, tile, sb, base);
-        if (!stored) {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) tile[base ^ voff<R>(v, sb)] = b[v];
-        }
-        continue;
-      }
-    } else {
-      for (int o = op0; o < op1; ++o) stored |= apply_op<R, true>(P.ops[o], a, a, mats, lane8, omask, tile, sb, base);
-    }
-    if (!stored) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) tile[base ^ voff<R>(v, sb)] = a[v];
-    }
-  }
-}
-
 constexpr int kMaxBuf = 4;
-
-template <int N>
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-
-// NT threads per CTA, all of them compute; the lanes of warp 0 also issue the
-// TMA copies.  Tiles cycle through `nbuf` shared-memory buffers: while tile i
-// is computed, tiles up to i + depth are loading and the stores of earlier
-// tiles are draining.  depth = nbuf - 2 for nbuf >= 3, else nbuf - 1, so the
-// buffer a load re-arms always held a tile every thread has finished with, and
-// its mbarrier is armed once per phase.
-template <int R, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-    tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
-                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
-  __shared__ volatile int abort_flag;
-
-  // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
-  double2* tiles = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const uint32_t tile_elems = 1u << P.M;
-  double2* smat = tiles + (size_t)nbuf * tile_elems;
-  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + i];
-  if (tid == 0) {
-    for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
-    abort_flag = 0;
-    fence_mbar_init();
-  }
-  __syncthreads();
-
-  const uint64_t ntiles = P.ntiles;
-  const uint64_t first = blockIdx.x;
-  const uint64_t cnt = (first < ntiles) ? (ntiles - 1 - first) / gridDim.x + 1 : 0;
-  const int depth = nbuf >= 3 ? nbuf - 2 : nbuf - 1;   // < nbuf
-
-  // ---- copy issue setup: every warp issues its share of a tile's copies
-  // (issues j = warp + NW * (lane + 32 r)); the tile mbarrier expects one
-  // arrival per warp.  Coordinates are linear in the disjoint address bits, so
-  // each lane keeps the offsets of its issues and adds the tile's base
-  // coordinates per tile.
-  constexpr int NW = NT / 32;
-  const int warp = tid >> 5;
-  const int nbox = P.nbox;
-  const int nissue = 1 << (P.nH - nbox);
-  const uint32_t box_elems = 1u << (P.c + nbox);
-  const uint32_t box_bytes = box_elems * 16u;
-  constexpr int kMaxPerLane = 1;   // nissue <= 32 * NW
-  int jc1[kMaxPerLane], jc3[kMaxPerLane], jc4[kMaxPerLane], jj[kMaxPerLane];
-  uint32_t my_bytes = 0;           // bytes of this warp's issues per tile
-#pragma unroll
-  for (int r = 0; r < kMaxPerLane; ++r) {
-    const int j = warp + NW * (lane + 32 * r);
-    jj[r] = j;
-    int c2;
-    if (j < nissue) chunk_coords(issue_offset(j, P), P, jc1[r], c2, jc3[r], jc4[r]);
-    else jc1[r] = jc3[r] = jc4[r] = 0;
-  }
-  for (int j = warp; j < nissue; j += NW) my_bytes += box_bytes;
-  int Hr[kMaxTileBits];
-#pragma unroll
-  for (int i = 0; i < kMaxTileBits; ++i) Hr[i] = P.H[i];
-  const int nH = P.nH, cb = P.c;
-  auto base_coords = [&](uint64_t t, int& c1, int& c3, int& c4) {
-    uint64_t x = t << cb;
-#pragma unroll
-    for (int i = 0; i < kMaxTileBits; ++i)
-      if (i < nH) {
-        const int h = Hr[i];
-        x = ((x >> h) << (h + 1)) | (x & ((1ULL << h) - 1));
-      }
-    int c2;
-    chunk_coords(x, P, c1, c2, c3, c4);
-  };
-  auto issue_load = [&](uint64_t i) {   // whole warp, converged
-    const int b = (int)(i % nbuf);
-    int c1, c3, c4;
-    base_coords(first + i * gridDim.x, c1, c3, c4);
-    double2* buf = tiles + (size_t)b * tile_elems;
-    if (lane == 0) mbar_arrive_expect_tx(&bar_loaded[b], my_bytes);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-      if (jj[r] < nissue)
-        tma_load_5d(buf + (size_t)jj[r] * box_elems, &tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r],
-                    &bar_loaded[b]);
-  };
-  auto issue_store = [&](uint64_t i) {  // whole warp; one bulk group per lane per tile
-    const int b = (int)(i % nbuf);
-    int c1, c3, c4;
-    base_coords(first + i * gridDim.x, c1, c3, c4);
-    double2* buf = tiles + (size_t)b * tile_elems;
-#pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-      if (jj[r] < nissue)
-        tma_store_5d(&tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r], buf + (size_t)jj[r] * box_elems);
-    bulk_commit();
-  };
-
-  uint64_t issued = 0;             // tiles whose loads have been issued
-  uint64_t first_unwaited = cnt;   // first tile whose load wait did not succeed
-  for (; issued < (uint64_t)depth && issued < cnt; ++issued) issue_load(issued);
-
-  for (uint64_t i = 0; i < cnt; ++i) {
-    const int b = (int)(i % nbuf);
-    // abort_flag is read after the previous iteration's barrier: uniform in the CTA
-    const bool ab = __shfl_sync(0xffffffffu, (int)abort_flag, 0) != 0;
-    if (i + depth < cnt && !ab) {
-      // buffer (i + depth) % nbuf last held tile i + depth - nbuf (finished by
-      // every thread: it is at most tile i - 1), whose store is followed by
-      // nbuf - depth - 1 later stores: wait only for that store's read
-      if (i + depth >= (uint64_t)nbuf) {
-        if (nbuf - depth - 1 >= 1) bulk_wait_read<1>();
-        else bulk_wait_read<0>();
-      }
-      __syncwarp();
-      issue_load(i + depth);
-      issued = i + depth + 1;
-    }
-    const bool ok = bounded_wait(&bar_loaded[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status, DEV_WAIT_LOADED);
-    const bool work = __syncthreads_and(ok && !abort_flag);
-    if (!work && first_unwaited == cnt) first_unwaited = i;
-    double2* buf = tiles + (size_t)b * tile_elems;
-    for (int s = 0; s < P.nstages; ++s) {
-      if (work) run_stage<R>(buf, P, s, smat, tid, NT);
-      __syncthreads();
-    }
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (work) issue_store(i);
-  }
-  // after an abort, let loads that were issued but never consumed land first
-  for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
-  bulk_wait_all();
-}
 
 // tile buffers + alignment slack + this pass's matrix block
 size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems) {
@@ -646,20 +40,8 @@ cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const dou
   const size_t smem = tile_pass_smem_bytes(d.M, nbuf, d.mat_elems);
   uint64_t grid = (uint64_t)num_sms * (uint64_t)(tl.ctas_per_sm < 1 ? 1 : tl.ctas_per_sm);
   if (grid > d.ntiles) grid = d.ntiles;
-  cudaError_t e;
-  auto go = [&](auto kern, int threads) {
-    cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (r != cudaSuccess) return r;
-    kern<<<(unsigned)grid, threads, smem, st>>>(tm, d, mats, dev_status, nbuf);
-    return cudaGetLastError();
-  };
-  if (d.R == 4) {
-    if (tl.consumers >= 256) e = go(tile_pass_kernel<4, 256, 1>, 256);
-    else e = go(tile_pass_kernel<4, 128, 2>, 128);
-  } else {
-    e = go(tile_pass_kernel<5, 128, 1>, 128);
-  }
-  return e;
+  if (d.R == 4) return launch_tile_r4(tm, d, mats, dev_status, nbuf, (unsigned)grid, smem, st);
+  return launch_tile_r5(tm, d, mats, dev_status, nbuf, (unsigned)grid, smem, st);
 }
 
 // ------------------------------------------------------------ tensor maps

@@ -18,7 +18,7 @@ enum DevErr : int {
 struct TileLaunch {
   int nbuf;                // shared-memory tile buffers per CTA (pipeline depth)
   int ctas_per_sm;         // resident CTAs per SM the grid is sized for
-  int consumers;           // consumer threads per CTA (128: two CTAs per SM; 256: one)
+  int consumers;           // threads per CTA (128)
 };
 
 // Encode the pass tensor map for `state` (2^nbits complex128).
@@ -28,6 +28,11 @@ int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d,
 cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
                              const TileLaunch& tl, int num_sms, cudaStream_t st);
 size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems);
+// one launcher per kernel instantiation (iq_tile_r4.cu, iq_tile_r5.cu)
+cudaError_t launch_tile_r4(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
+                           unsigned grid, size_t smem, cudaStream_t st);
+cudaError_t launch_tile_r5(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
+                           unsigned grid, size_t smem, cudaStream_t st);
 
 // Simple path: one operation straight in global memory (k = 1..5, LSB-first bits).
 struct SimpleOp {

@@ -237,14 +237,14 @@ struct Engine {
     if (!cuda_ok(cudaEventCreateWithFlags(&pool_ev, cudaEventDisableTiming), "cudaEventCreate")) return false;
     cudaMemsetAsync(d_status, 0, sizeof(int), stream);
     sp.nbits = nbits;
-    tl.consumers = env_int("IQ_CONSUMERS", 128);
-    sp.M = env_int("IQ_TILE_BITS", tl.consumers >= 256 ? 12 : 11);
+    tl.consumers = 128;
+    sp.M = env_int("IQ_TILE_BITS", 11);
     sp.c = env_int("IQ_CHUNK_BITS", 5);
     sp.R = 4;
     sp.max_stages = env_int("IQ_MAX_STAGES", 8);
     sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
-    tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", tl.consumers >= 256 ? 1 : 2);
+    tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
     eager = env_int("IQ_EAGER", 0);
     return reset_state();
   }
@@ -1059,7 +1059,7 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; }
   else if (!strcmp(key, "nbuf")) { if (iv < 1 || iv > 4) return -1; e->tl.nbuf = iv; }
   else if (!strcmp(key, "ctas_per_sm")) { if (iv < 1 || iv > 4) return -1; e->tl.ctas_per_sm = iv; }
-  else if (!strcmp(key, "consumers")) { if (iv != 128 && iv != 256) return -1; e->tl.consumers = iv; }
+  else if (!strcmp(key, "consumers")) { if (iv != 128) return -1; e->tl.consumers = iv; }
   else if (!strcmp(key, "eager")) e->eager = iv ? 1 : 0;
   else if (!strcmp(key, "fuse")) e->fuse = iv ? 1 : 0;
   else if (!strcmp(key, "flush_ops")) { if (iv < 1) return -1; e->flush_ops = iv; }

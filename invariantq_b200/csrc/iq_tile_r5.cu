@@ -1,0 +1,17 @@
+// iq_tile_r5.cu -- instantiation of the tile-pass kernel with R = 5 register
+// slots (32 amplitudes per thread), 128 threads per CTA, 1 CTA(s) per SM.  Kept in
+// its own translation unit so the instantiations compile in parallel.
+#include "iq_tile.cuh"
+
+namespace iqb {
+
+cudaError_t launch_tile_r5(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
+                          unsigned grid, size_t smem, cudaStream_t st) {
+  auto kern = tile_pass_kernel<5, 128, 1>;
+  cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (r != cudaSuccess) return r;
+  kern<<<grid, 128, smem, st>>>(tm, d, mats, dev_status, nbuf);
+  return cudaGetLastError();
+}
+
+}  // namespace iqb
