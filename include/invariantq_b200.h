@@ -177,6 +177,65 @@ int iq_handle_profile_read(void* h, double* ms_out, size_t max);
 #define IQ_NOALLOC_MAX_QUBITS 34
 int iq_statevector_expval_z_all_noalloc(const void* d_amps, size_t num_qubits, double* d_out, void* stream);
 
+/* ---- Adjoint-method gradients (no counterpart in the reference; the energy
+ * they differentiate is the TFIM expectation of invariantq/algorithms/vqe.py:44-79).
+ *
+ * A parametrised circuit on num_qubits qubits, starting from |0...0>: gate i
+ * has kind kinds[i] (IQ_GATE_*), qubit q0[i] (control q0, target q1 for CX;
+ * the two qubits of CZ) and, for the rotation kinds, first parameter index
+ * param_index[i].  RX/RY/RZ(t) = exp(-i t P / 2); P(l) = diag(1, e^{i l});
+ * U3 reads parameters p, p+1, p+2 as (theta, phi, lambda) with the
+ * reference's U3 matrix.  H = sum_t coeffs[t] P_t with P_t the num_qubits
+ * characters paulis[t * num_qubits .. +num_qubits) ('I','X','Y','Z';
+ * character q acts on qubit q).  Outputs: energy <psi|H|psi> and dE/dparam
+ * for every parameter (parameters read by several gates sum their terms). */
+#define IQ_GATE_RX 1
+#define IQ_GATE_RY 2
+#define IQ_GATE_RZ 3
+#define IQ_GATE_U3 4
+#define IQ_GATE_P  5
+#define IQ_GATE_CZ 6
+#define IQ_GATE_CX 7
+#define IQ_GATE_H  8
+#define IQ_GATE_X  9
+#define IQ_GATE_SX 10
+
+typedef struct iq_adjoint_circuit {
+  size_t num_qubits;
+  size_t num_ops;
+  const int* kinds;
+  const int* q0;
+  const int* q1;
+  const int* param_index;
+  size_t num_params;        /* parameters per set (columns of params) */
+  size_t num_sets;          /* parameter sets evaluated for this circuit */
+  const double* params;     /* num_sets x num_params, row-major */
+  size_t num_terms;
+  const double* coeffs;     /* num_terms */
+  const char* paulis;       /* num_terms x num_qubits */
+  double* energy_out;       /* num_sets */
+  double* grad_out;         /* num_sets x num_params (unused by iq_ansatz_energy) */
+} iq_adjoint_circuit;
+
+/* One circuit, one parameter set.  Returns 0, or -1 with iq_last_error set. */
+int iq_adjoint_gradient(size_t num_qubits, size_t num_ops, const int* kinds, const int* q0, const int* q1,
+                        const int* param_index, size_t num_params, const double* params, size_t num_terms,
+                        const double* coeffs, const char* paulis, double* energy_out, double* grad_out);
+/* Every parameter set of every circuit, run concurrently on num_streams CUDA
+ * streams (<= 0: IQ_ADJOINT_STREAMS or 8), each with its own device workspace
+ * sized for the largest circuit; fewer streams when the workspaces would not
+ * fit in device memory.  Returns 0, or -1 with iq_last_error set. */
+int iq_adjoint_gradient_batch(const iq_adjoint_circuit* circuits, size_t num_circuits, int num_streams);
+/* Energies only (grad_out unused): the forward circuit and <psi|H|psi> for each
+ * parameter set of one circuit, one set after another on one stream -- the
+ * plain path a parameter-shift gradient evaluates 2 x num_params times. */
+int iq_ansatz_energy(const iq_adjoint_circuit* circuit);
+/* Counters of the calling thread's last adjoint / energy call: out[0] jobs,
+ * [1] forward passes, [2] backward passes, [3] kernel launches, [4] algorithmic
+ * HBM bytes of the passes, [5] host preparation ms (summed over workers),
+ * [6] wall ms, [7] streams used.  Returns the number of counters (8). */
+int iq_adjoint_stats(double* out, size_t n);
+
 /* Density-matrix additions. */
 int iq_density_matrix_flush(void* dm);
 /* Kraus channel on two qubits: num_kraus 4x4 matrices, q0 = most significant

@@ -20,6 +20,16 @@ _v = ctypes.c_void_p
 _sz = ctypes.c_size_t
 _d = ctypes.c_double
 _i = ctypes.c_int
+c_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class AdjointCircuit(ctypes.Structure):
+    """iq_adjoint_circuit (include/invariantq_b200.h)."""
+    _fields_ = [("num_qubits", _sz), ("num_ops", _sz), ("kinds", c_ip), ("q0", c_ip), ("q1", c_ip),
+                ("param_index", c_ip), ("num_params", _sz), ("num_sets", _sz), ("params", c_dp),
+                ("num_terms", _sz), ("coeffs", c_dp), ("paulis", ctypes.c_char_p), ("energy_out", c_dp),
+                ("grad_out", c_dp)]
+
 
 SIGNATURES = {
     # reference ABI: state vector
@@ -98,6 +108,11 @@ SIGNATURES = {
     "iq_program_info": ([_v, c_dp, _sz], _i),
     "iq_program_free": ([_v], None),
     "iq_statevector_expval_z_all_noalloc": ([_v, _sz, _v, _v], _i),
+    "iq_adjoint_gradient": ([_sz, _sz, c_ip, c_ip, c_ip, c_ip, _sz, c_dp, _sz, c_dp, ctypes.c_char_p, c_dp, c_dp],
+                            _i),
+    "iq_adjoint_gradient_batch": ([ctypes.POINTER(AdjointCircuit), _sz, _i], _i),
+    "iq_ansatz_energy": ([ctypes.POINTER(AdjointCircuit)], _i),
+    "iq_adjoint_stats": ([c_dp, _sz], _i),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),
     "iq_density_matrix_get_diagonal": ([_v, c_dp], None),

@@ -34,14 +34,20 @@ size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems) {
 }
 
 
-cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
-                             const TileLaunch& tl, int num_sms, cudaStream_t st) {
-  const int nbuf = tl.nbuf < 1 ? 1 : (tl.nbuf > kMaxBuf ? kMaxBuf : tl.nbuf);
-  const size_t smem = tile_pass_smem_bytes(d.M, nbuf, d.mat_elems);
+unsigned tile_pass_grid(const PassDesc& d, const TileLaunch& tl, int num_sms) {
   uint64_t grid = (uint64_t)num_sms * (uint64_t)(tl.ctas_per_sm < 1 ? 1 : tl.ctas_per_sm);
   if (grid > d.ntiles) grid = d.ntiles;
-  if (d.R == 4) return launch_tile_r4(tm, d, mats, dev_status, nbuf, (unsigned)grid, smem, st);
-  return launch_tile_r5(tm, d, mats, dev_status, nbuf, (unsigned)grid, smem, st);
+  return (unsigned)grid;
+}
+
+cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
+                             const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials) {
+  const int nbuf = tl.nbuf < 1 ? 1 : (tl.nbuf > kMaxBuf ? kMaxBuf : tl.nbuf);
+  const size_t smem = tile_pass_smem_bytes(d.M, nbuf, d.mat_elems);
+  const unsigned grid = tile_pass_grid(d, tl, num_sms);
+  if (d.ngrad && !grad_partials) return cudaErrorInvalidValue;
+  if (d.R == 4) return launch_tile_r4(tm, d, mats, dev_status, nbuf, grid, smem, st, grad_partials);
+  return launch_tile_r5(tm, d, mats, dev_status, nbuf, grid, smem, st, grad_partials);
 }
 
 // ------------------------------------------------------------ tensor maps
@@ -547,6 +553,63 @@ cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, i
   const uint64_t kd = 1ULL << k;
   const uint64_t npairs = kd * (kd + 1) / 2;
   partial_trace_kernel<<<(unsigned)npairs, 256, 0, st>>>(s, a, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------- adjoint gradients
+
+// lambda = H psi written next to psi in the joint array (joint[2x] = psi[x],
+// joint[2x + 1] = lambda[x]; skipped when joint is null) and the block sums of
+// Re conj(psi) lambda.
+// H = sum over groups g of sum over terms t of c_t (-1)^popc((x ^ xmask_g) & zmask_t)
+// psi[x ^ xmask_g]: Pauli strings sharing their X part share one gather.
+__global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64_t dim, HamTerms h,
+                                         const uint64_t* __restrict__ zmask, const double2* __restrict__ coef,
+                                         double2* __restrict__ joint, double* __restrict__ partials) {
+  double e = 0.0;
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 px = psi[x];
+    double2 lam = make_double2(0.0, 0.0);
+    for (int g = 0; g < h.ngroups; ++g) {
+      const uint64_t src = x ^ h.xmask[g];
+      const double2 a = (h.xmask[g] == 0) ? px : psi[src];
+      double2 f = make_double2(0.0, 0.0);
+      for (int t = h.first[g]; t < h.first[g + 1]; ++t) {
+        const double2 c = coef[t];
+        if (__popcll(src & zmask[t]) & 1) { f.x -= c.x; f.y -= c.y; }
+        else { f.x += c.x; f.y += c.y; }
+      }
+      lam = cfma(lam, f, a);
+    }
+    if (joint) {
+      joint[2 * x] = px;
+      joint[2 * x + 1] = lam;
+    }
+    e += px.x * lam.x + px.y * lam.y;
+  }
+  e = block_sum(e);
+  if (threadIdx.x == 0) partials[blockIdx.x] = e;
+}
+
+cudaError_t launch_hamiltonian_joint(const double2* psi, int n, const HamTerms& h, const uint64_t* zmask,
+                                     const double2* coef, double2* joint, double* partials, double* energy,
+                                     cudaStream_t st) {
+  hamiltonian_joint_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(psi, 1ULL << n, h, zmask, coef, joint, partials);
+  final_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, energy);
+  return cudaGetLastError();
+}
+
+// out[r] = sum_c in[r * cols + c], in order (one block per row)
+__global__ void row_sum_kernel(const double* __restrict__ in, int cols, double* __restrict__ out) {
+  double v = 0.0;
+  for (int c = threadIdx.x; c < cols; c += blockDim.x) v += in[(size_t)blockIdx.x * cols + c];
+  v = block_sum(v);
+  if (threadIdx.x == 0) out[blockIdx.x] = v;
+}
+
+cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st) {
+  if (rows <= 0) return cudaSuccess;
+  row_sum_kernel<<<rows, 256, 0, st>>>(in, cols, out);
   return cudaGetLastError();
 }
 

@@ -25,14 +25,17 @@ struct TileLaunch {
 int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d, char* err, size_t errlen);
 
 // Launch one tile pass.  `mats` is the device copy of the flush's matrix pool.
+// grad_partials: [gradient term][CTA] partial sums of the pass's OP_GRAD2 terms (or null)
 cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
-                             const TileLaunch& tl, int num_sms, cudaStream_t st);
+                             const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials = nullptr);
 size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems);
 // one launcher per kernel instantiation (iq_tile_r4.cu, iq_tile_r5.cu)
 cudaError_t launch_tile_r4(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
-                           unsigned grid, size_t smem, cudaStream_t st);
+                           unsigned grid, size_t smem, cudaStream_t st, double* grad_partials);
 cudaError_t launch_tile_r5(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
-                           unsigned grid, size_t smem, cudaStream_t st);
+                           unsigned grid, size_t smem, cudaStream_t st, double* grad_partials);
+// grid size the tile pass uses for `d` (the stride of its gradient partials)
+unsigned tile_pass_grid(const PassDesc& d, const TileLaunch& tl, int num_sms);
 
 // Simple path: one operation straight in global memory (k = 1..5, LSB-first bits).
 struct SimpleOp {
@@ -80,7 +83,24 @@ cudaError_t launch_block_search(const double2* s, int bbits, const uint64_t* blk
 // rho_A[r][c] = sum_env a[idx(r,env)] conj(a[idx(c,env)]), keep[] LSB-first (k <= 12)
 cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, int k, double2* out, cudaStream_t st);
 
+// ---- adjoint gradients ----
+// Pauli terms grouped by their X part: group g covers terms [first[g], first[g+1]).
+constexpr int kMaxHamGroups = 64;
+struct HamTerms {
+  int ngroups;
+  uint64_t xmask[kMaxHamGroups];
+  int first[kMaxHamGroups + 1];
+};
+// joint[2x] = psi[x], joint[2x+1] = (H psi)[x] for x < 2^n (when joint is not null);
+// *energy = Re <psi|H|psi>
+cudaError_t launch_hamiltonian_joint(const double2* psi, int n, const HamTerms& h, const uint64_t* zmask,
+                                     const double2* coef, double2* joint, double* partials, double* energy,
+                                     cudaStream_t st);
+cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st);
+
 // Record an error for iq_last_error (defined in iq_runtime.cu).
 void record_error(int code, const char* msg);
+// Add to the iq_kernel_launches counter (defined in iq_runtime.cu).
+void count_launches(uint64_t n);
 
 }  // namespace iqb

@@ -35,6 +35,7 @@ constexpr int kMaxStages = 24;
 constexpr int kMaxPassOps = 160;
 constexpr int kMaxK = 5;           // widest dense block the kernels apply
 constexpr int kSmemMatElems = 1024; // per-pass matrix block kept in shared memory (16 KiB)
+constexpr int kMaxPassGrads = 64;   // gradient terms accumulated by one pass
 
 enum OpKind : uint8_t {
   OP_NONE = 0,
@@ -45,6 +46,9 @@ enum OpKind : uint8_t {
   OP_M1R = 5,   // monomial 2x2 (permutation + phases), register slot a
   OP_M1L = 6,   // monomial 2x2, lane bit a
   OP_M2R = 7,   // monomial 4x4, register slots a (bit 0) and b (bit 1)
+  OP_GRAD2 = 8, // adjoint step on slots a (psi/lambda select bit) and b (qubit bit): add
+                // Im<lambda|P|psi> (P = X, Y, Z for `perm` = 0, 1, 2) to gradient term
+                // `gidx`, then apply the 2x2 matrix at `mat` to the qubit for both halves
 };
 
 // flags
@@ -57,7 +61,7 @@ struct OpDesc {          // 16 bytes
   uint8_t flags;
   uint8_t pad0, pad1;
   uint32_t mat;          // offset (complex elements) into the flush's matrix buffer
-  uint32_t pad2;
+  uint32_t gidx;         // OP_GRAD2: gradient term index (global; see PassDesc::grad_base)
 };
 
 struct StageDesc {       // 28 bytes
@@ -77,6 +81,8 @@ struct PassDesc {
   uint32_t nops, pad2;
   uint32_t mat_base;             // this pass's matrix block in the flush's matrix pool
   uint32_t mat_elems;            // complex elements in the block (ops' `mat` are relative to it)
+  uint32_t grad_base;            // gradient term index of the pass's first OP_GRAD2
+  uint32_t ngrad;                // OP_GRAD2 terms in the pass (consecutive indices, <= kMaxPassGrads)
   StageDesc st[kMaxStages];
   OpDesc ops[kMaxPassOps];
 };
@@ -90,6 +96,9 @@ struct SchedOp {
   uint8_t unit;          // monomial with unit phases
   uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
   uint32_t dense;        // complex offset of the dense 2^k x 2^k matrix (always present)
+  uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
+  uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
+  uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
 };
 
 struct SchedParams {
@@ -212,6 +221,29 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
 // every op's `mat` relative to its pass block, which the kernel stages in
 // shared memory.
 void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::vector<cplx64>& packed);
+
+// ---- adjoint-method gradients ----------------------------------------------
+// Gate kinds of a parametrised circuit (the values of the C ABI's IQ_GATE_*).
+enum GateKind : int {
+  GATE_RX = 1, GATE_RY = 2, GATE_RZ = 3, GATE_U3 = 4, GATE_P = 5,   // parametrised (U3 takes 3)
+  GATE_CZ = 6, GATE_CX = 7, GATE_H = 8, GATE_X = 9, GATE_SX = 10    // fixed
+};
+struct AnsatzOp {
+  int kind;
+  int q0, q1;     // q1 only for CZ / CX (CX: q0 control, q1 target)
+  int param;      // index of the (first) parameter, -1 for fixed gates
+};
+// Validate an ansatz; returns the number of parameters it reads (max index + 1) or -1.
+int ansatz_check(int n, const std::vector<AnsatzOp>& ops, std::string& err);
+// Forward circuit on an n-bit state vector: ops appended to `out` (matrices to `pool`).
+void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
+                    std::vector<cplx64>& pool);
+// Backward sweep on the joint array of n + 1 bits (bit 0 selects psi (0) or
+// lambda = H psi (1), bit q + 1 is qubit q): for every gate from last to first,
+// an adjoint step (gradient term + inverse rotation) per rotation angle, or the
+// inverse of a fixed gate.  grad_param[t] is the parameter gradient term t adds to.
+void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param);
 // Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
 // and fills perm/phases/unit if every row and column holds exactly one nonzero.
 int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);

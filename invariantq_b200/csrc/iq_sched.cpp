@@ -15,14 +15,19 @@
 #include <cmath>
 #include <cstring>
 #include <array>
+#include <complex>
 #include <set>
 
 namespace iqb {
 
 // complex elements of an operation's matrix data (dense 4^k, monomial 2^k phases)
-int op_mat_elems(const SchedOp& op) { return op.mono ? (1 << op.k) : (1 << (2 * op.k)); }
+int op_mat_elems(const SchedOp& op) {
+  if (op.grad) return 4;
+  return op.mono ? (1 << op.k) : (1 << (2 * op.k));
+}
 
 double op_cost(const SchedOp& op) {
+  if (op.grad) return 24.0;   // 2x2 on both halves plus the gradient products
   if (op.mono) return op.unit ? 0.25 : 4.0;
   return 4.0 * double(1u << op.k);
 }
@@ -111,6 +116,24 @@ struct PassBuilder {
     return true;
   }
   bool place(int idx, const SchedOp& op) {
+    if (op.grad) {
+      // adjoint steps want the psi / lambda select bit in register slot 0
+      if (!stages.empty()) {
+        Stage trial = stages.back();
+        if (!trial.dk && trial.nS > 0 && trial.S[0] == op.q[0] && tryAdd(trial, op)) {
+          trial.ops.push_back(idx);
+          stages.back() = trial;
+          return true;
+        }
+      }
+      if ((int)stages.size() >= p.max_stages) return false;
+      Stage s;
+      s.S[s.nS++] = op.q[0];
+      if (!tryAdd(s, op)) return false;
+      s.ops.push_back(idx);
+      stages.push_back(s);
+      return true;
+    }
     if (op.k >= 3) {
       if (op.k > p.R) return false;
       if ((int)stages.size() >= p.max_stages) return false;
@@ -244,6 +267,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     std::vector<int> taken;
     double cost = 0.0;
     int mat_elems = 0;
+    int ngrad = 0;
     for (;;) {
       bool progress = true;
       while (progress) {
@@ -254,10 +278,11 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
           const double oc = op_cost(o);
           if ((opmask(o) & ~local) == 0 && (int)taken.size() < kMaxPassOps &&
               mat_elems + op_mat_elems(o) <= kSmemMatElems && (taken.empty() || cost + oc <= p.budget) &&
-              pb.place(i, o)) {
+              (!o.grad || ngrad < kMaxPassGrads) && pb.place(i, o)) {
             taken.push_back(i);
             cost += oc;
             mat_elems += op_mat_elems(o);
+            ngrad += o.grad ? 1 : 0;
             it = ready.erase(it);
             retire(i);
             progress = true;
@@ -360,9 +385,14 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         } else if (o.k == 2) {
           const int j0 = pos[o.q[0]], j1 = pos[o.q[1]];
           if (slot_of[j0] < 0 || slot_of[j1] < 0) { err = "internal: 2q operation outside slots"; return -1; }
-          od.kind = o.mono ? OP_M2R : OP_D2R;
+          od.kind = o.grad ? OP_GRAD2 : (o.mono ? OP_M2R : OP_D2R);
           od.a = (uint8_t)slot_of[j0];
           od.b = (uint8_t)slot_of[j1];
+          if (o.grad) {
+            od.perm = o.gen;
+            od.flags = 0;
+            od.gidx = o.gidx;
+          }
         } else {
           for (int t = 0; t < o.k; ++t)
             if (slot_of[pos[o.q[t]]] != t) { err = "internal: dense block slots out of order"; return -1; }
@@ -372,6 +402,18 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
       sd.op1 = (uint16_t)nout;
     }
     d.nops = (uint32_t)nout;
+    d.ngrad = 0;
+    d.grad_base = 0;
+    for (int i : taken)
+      if (ops[i].grad) {
+        if (d.ngrad == 0 || ops[i].gidx < d.grad_base) d.grad_base = ops[i].gidx;
+        ++d.ngrad;
+      }
+    for (int i : taken)
+      if (ops[i].grad && (ops[i].gidx < d.grad_base || ops[i].gidx >= d.grad_base + d.ngrad)) {
+        err = "internal: gradient terms of a pass are not consecutive";
+        return -1;
+      }
     plan.nsrc = (int)taken.size();
     plan.cost = cost;
     out.push_back(plan);
@@ -443,7 +485,7 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
   };
   for (size_t i = 0; i < ops.size(); ++i) {
     const SchedOp& o = ops[i];
-    if (o.k >= 3) {
+    if (o.k >= 3 || o.grad) {   // wide blocks and adjoint steps pass through unchanged
       for (int j = 0; j < o.k; ++j) { open[o.q[j]] = -1; last[o.q[j]] = (int)blocks.size(); }
       Block b;
       b.k = 0;
@@ -568,6 +610,154 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
   return out;
 }
 
+// ------------------------------------------------------------ adjoint builder
+namespace {
+
+using cdd = std::complex<double>;
+
+void push_op(std::vector<SchedOp>& out, std::vector<cplx64>& pool, int k, const int* q, const cdd* m) {
+  SchedOp o{};
+  o.k = (uint8_t)k;
+  for (int i = 0; i < k; ++i) o.q[i] = (uint8_t)q[i];
+  const int d = 1 << k;
+  o.dense = o.mat = (uint32_t)pool.size();
+  double flat[32];
+  for (int i = 0; i < d * d; ++i) {
+    pool.push_back({m[i].real(), m[i].imag()});
+    flat[2 * i] = m[i].real();
+    flat[2 * i + 1] = m[i].imag();
+  }
+  double ph[8];
+  uint8_t perm = 0, unit = 0;
+  if (classify_monomial(flat, k, &perm, ph, &unit)) {
+    o.mono = 1;
+    o.perm = perm;
+    o.unit = unit;
+    o.mat = (uint32_t)pool.size();
+    for (int i = 0; i < d; ++i) pool.push_back({ph[2 * i], ph[2 * i + 1]});
+  }
+  out.push_back(o);
+}
+
+// exp(-i theta P / 2) for P = X (g 0), Y (1), Z (2)
+void rotation(int g, double th, cdd* m) {
+  const double c = std::cos(th / 2.0), s = std::sin(th / 2.0);
+  const cdd I(0.0, 1.0);
+  if (g == 0) { m[0] = c; m[1] = -I * s; m[2] = -I * s; m[3] = c; }
+  else if (g == 1) { m[0] = c; m[1] = -s; m[2] = s; m[3] = c; }
+  else { m[0] = std::exp(-I * (th / 2.0)); m[1] = 0.0; m[2] = 0.0; m[3] = std::exp(I * (th / 2.0)); }
+}
+
+void dagger2(const cdd* m, cdd* o) {
+  o[0] = std::conj(m[0]); o[1] = std::conj(m[2]); o[2] = std::conj(m[1]); o[3] = std::conj(m[3]);
+}
+
+// the rotations a parametrised gate is made of, in forward order: (generator, parameter)
+int rotations_of(const AnsatzOp& op, int gen[3], int par[3]) {
+  switch (op.kind) {
+    case GATE_RX: gen[0] = 0; par[0] = op.param; return 1;
+    case GATE_RY: gen[0] = 1; par[0] = op.param; return 1;
+    case GATE_RZ: case GATE_P: gen[0] = 2; par[0] = op.param; return 1;
+    // U3(theta, phi, lambda) = e^{i (phi + lambda) / 2} Rz(phi) Ry(theta) Rz(lambda)
+    case GATE_U3: gen[0] = 2; par[0] = op.param + 2; gen[1] = 1; par[1] = op.param; gen[2] = 2; par[2] = op.param + 1;
+      return 3;
+    default: return 0;
+  }
+}
+
+void fixed_matrix(const AnsatzOp& op, int& k, int q[2], cdd* m) {
+  const double r = 1.0 / std::sqrt(2.0);
+  const cdd I(0.0, 1.0);
+  for (int i = 0; i < 16; ++i) m[i] = 0.0;
+  switch (op.kind) {
+    case GATE_H: k = 1; q[0] = op.q0; m[0] = r; m[1] = r; m[2] = r; m[3] = -r; return;
+    case GATE_X: k = 1; q[0] = op.q0; m[1] = 1.0; m[2] = 1.0; return;
+    case GATE_SX: k = 1; q[0] = op.q0; m[0] = 0.5 * (1.0 + I); m[1] = 0.5 * (1.0 - I); m[2] = 0.5 * (1.0 - I);
+      m[3] = 0.5 * (1.0 + I); return;
+    case GATE_CZ: k = 2; q[0] = op.q1; q[1] = op.q0; m[0] = 1.0; m[5] = 1.0; m[10] = 1.0; m[15] = -1.0; return;
+    case GATE_CX:   // local bit 1 = control q0, bit 0 = target q1
+      k = 2; q[0] = op.q1; q[1] = op.q0; m[0] = 1.0; m[5] = 1.0; m[11] = 1.0; m[14] = 1.0; return;
+    default: k = 0; return;
+  }
+}
+
+}  // namespace
+
+int ansatz_check(int n, const std::vector<AnsatzOp>& ops, std::string& err) {
+  int np = 0;
+  for (const AnsatzOp& o : ops) {
+    if (o.kind < GATE_RX || o.kind > GATE_SX) { err = "unknown gate kind"; return -1; }
+    if (o.q0 < 0 || o.q0 >= n) { err = "qubit out of range"; return -1; }
+    if (o.kind == GATE_CZ || o.kind == GATE_CX) {
+      if (o.q1 < 0 || o.q1 >= n || o.q1 == o.q0) { err = "invalid second qubit"; return -1; }
+    }
+    if (o.kind <= GATE_P) {
+      if (o.param < 0) { err = "parametrised gate without a parameter index"; return -1; }
+      np = std::max(np, o.param + (o.kind == GATE_U3 ? 3 : 1));
+    }
+  }
+  return np;
+}
+
+void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
+                    std::vector<cplx64>& pool) {
+  (void)n;
+  for (const AnsatzOp& o : ops) {
+    int gen[3], par[3];
+    const int nr = rotations_of(o, gen, par);
+    if (nr) {
+      for (int r = 0; r < nr; ++r) {
+        cdd m[4];
+        rotation(gen[r], params[par[r]], m);
+        const int q[1] = {o.q0};
+        push_op(out, pool, 1, q, m);
+      }
+      continue;
+    }
+    int k, q[2];
+    cdd m[16];
+    fixed_matrix(o, k, q, m);
+    push_op(out, pool, k, q, m);
+  }
+}
+
+void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param) {
+  (void)n;
+  for (size_t i = ops.size(); i-- > 0;) {
+    const AnsatzOp& o = ops[i];
+    int gen[3], par[3];
+    const int nr = rotations_of(o, gen, par);
+    if (nr) {
+      for (int r = nr - 1; r >= 0; --r) {   // last rotation of the gate first
+        cdd m[4], md[4];
+        rotation(gen[r], params[par[r]], m);
+        dagger2(m, md);
+        SchedOp g{};
+        g.k = 2;
+        g.q[0] = 0;                       // psi / lambda select bit
+        g.q[1] = (uint8_t)(o.q0 + 1);
+        g.grad = 1;
+        g.gen = (uint8_t)gen[r];
+        g.gidx = (uint32_t)grad_param.size();
+        g.dense = g.mat = (uint32_t)pool.size();
+        for (int j = 0; j < 4; ++j) pool.push_back({md[j].real(), md[j].imag()});
+        out.push_back(g);
+        grad_param.push_back(par[r]);
+      }
+      continue;
+    }
+    int k, q[2];
+    cdd m[16], md[16];
+    fixed_matrix(o, k, q, m);
+    const int d = 1 << k;
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c) md[r * d + c] = std::conj(m[c * d + r]);
+    int qj[2] = {q[0] + 1, q[1] + 1};
+    push_op(out, pool, k, qj, md);
+  }
+}
+
 void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::vector<cplx64>& packed) {
   packed.clear();
   for (auto& pl : plans) {
@@ -576,7 +766,7 @@ void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::v
     for (uint32_t i = 0; i < d.nops; ++i) {
       OpDesc& od = d.ops[i];
       const bool mono = od.kind == OP_M1R || od.kind == OP_M1L || od.kind == OP_M2R;
-      const uint32_t n = mono ? (1u << od.k) : (1u << (2 * od.k));
+      const uint32_t n = od.kind == OP_GRAD2 ? 4u : (mono ? (1u << od.k) : (1u << (2 * od.k)));
       const uint32_t rel = (uint32_t)packed.size() - base;
       packed.insert(packed.end(), pool + od.mat, pool + od.mat + n);
       od.mat = rel;

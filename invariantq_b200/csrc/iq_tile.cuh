@@ -361,6 +361,33 @@ __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
+// Adjoint step on slot 0 (psi / lambda select bit) and slot B (the qubit):
+// returns this thread's share of Im<lambda| P |psi> for generator P (GEN 0 = X,
+// 1 = Y, 2 = Z), then applies the 2x2 matrix (the inverse gate) to the qubit
+// in both halves.  Inputs are read before outputs are written (in-place safe).
+template <int R, int B, int GEN>
+__device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
+  const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
+  double acc = 0.0;
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & (1 | (1 << B))) continue;
+    const double2 p0 = s[v], p1 = s[v | (1 << B)], l0 = s[v | 1], l1 = s[v | 1 | (1 << B)];
+    if (GEN == 0) {         // X: (P psi)_0 = psi_1, (P psi)_1 = psi_0
+      acc += (l0.x * p1.y - l0.y * p1.x) + (l1.x * p0.y - l1.y * p0.x);
+    } else if (GEN == 1) {  // Y: (P psi)_0 = -i psi_1, (P psi)_1 = i psi_0
+      acc += (l1.x * p0.x + l1.y * p0.y) - (l0.x * p1.x + l0.y * p1.y);
+    } else {                // Z: (P psi)_0 = psi_0, (P psi)_1 = -psi_1
+      acc += (l0.x * p0.y - l0.y * p0.x) - (l1.x * p1.y - l1.y * p1.x);
+    }
+    d[v] = cfma(cmul(u0, p0), u1, p1);
+    d[v | (1 << B)] = cfma(cmul(u2, p0), u3, p1);
+    d[v | 1] = cfma(cmul(u0, l0), u1, l1);
+    d[v | 1 | (1 << B)] = cfma(cmul(u2, l0), u3, l1);
+  }
+  return acc;
+}
+
 // ------------------------------------------------------- runtime dispatch
 
 template <int R, int S = 0>
@@ -423,14 +450,43 @@ __device__ __forceinline__ void disp_dkr(int k, const double2 (&a)[1 << R], cons
   }
 }
 
+template <int R, int GEN, int B = 1>
+__device__ __forceinline__ double disp_grad2_b(int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R],
+                                               const double2* m) {
+  if constexpr (B < R) {
+    if (sb == B) return grad2<R, B, GEN>(s, d, m);
+    return disp_grad2_b<R, GEN, B + 1>(sb, s, d, m);
+  }
+  return 0.0;
+}
+
+// the octet's eight lanes hold the same registers of eight tile rows: sum
+// their shares, and one lane adds it to the CTA's accumulator in shared memory
+__device__ __forceinline__ void grad_accumulate(double acc, double* slot, int lane8, unsigned omask) {
+  acc += __shfl_xor_sync(omask, acc, 1, 8);
+  acc += __shfl_xor_sync(omask, acc, 2, 8);
+  acc += __shfl_xor_sync(omask, acc, 4, 8);
+  if (lane8 == 0) atomicAdd(slot, acc);
+}
+
 // Apply one operation from s to d; returns true when it wrote the tile itself.
 template <int R, bool IP>
 __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 << R], double2 (&d)[1 << R],
                                          const double2* mats, int lane8, unsigned omask, double2* tile,
-                                         const uint32_t (&sb)[R], uint32_t base) {
+                                         const uint32_t (&sb)[R], uint32_t base, double* sgrad,
+                                         uint32_t grad_base) {
   const double2* m = mats + od.mat;
   const bool unit = od.flags & OPF_UNIT_PHASE;
   switch (od.kind) {
+    case OP_GRAD2: {
+      // the planner puts the select bit in slot 0
+      double acc;
+      if (od.perm == 0) acc = disp_grad2_b<R, 0>(od.b, s, d, m);
+      else if (od.perm == 1) acc = disp_grad2_b<R, 1>(od.b, s, d, m);
+      else acc = disp_grad2_b<R, 2>(od.b, s, d, m);
+      grad_accumulate(acc, sgrad + (od.gidx - grad_base), lane8, omask);
+      break;
+    }
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
     case OP_D2R: disp_d2r<R, IP>(od.a, od.b, s, d, m); break;
@@ -447,7 +503,7 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
 // lives in shared-memory slot swz(j); every offset below is kept swizzled.
 template <int R>
 __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int s, const double2* mats,
-                                          int ctid, int ncons) {
+                                          int ctid, int ncons, double* sgrad) {
   constexpr int NV = 1 << R;
   const StageDesc& sd = P.st[s];
   const int lane8 = ctid & 7;
@@ -472,16 +528,16 @@ __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int 
       // (two inlined dispatch sites only)
       double2 b[NV];
       for (int o = op0; o < op1; o += 2) {
-        stored |= apply_op<R, false>(P.ops[o], a, b, mats, lane8, omask, tile, sb, base);
+        stored |= apply_op<R, false>(P.ops[o], a, b, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
         if (o + 1 < op1) {
-          stored |= apply_op<R, false>(P.ops[o + 1], b, a, mats, lane8, omask, tile, sb, base);
+          stored |= apply_op<R, false>(P.ops[o + 1], b, a, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
         } else if (!stored) {
 #pragma unroll
           for (int v = 0; v < NV; ++v) a[v] = b[v];
         }
       }
     } else {
-      for (int o = op0; o < op1; ++o) stored |= apply_op<R, true>(P.ops[o], a, a, mats, lane8, omask, tile, sb, base);
+      for (int o = op0; o < op1; ++o) stored |= apply_op<R, true>(P.ops[o], a, a, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
     }
     if (!stored) {
 #pragma unroll
@@ -506,9 +562,11 @@ __device__ __forceinline__ void bulk_wait_read() {
 template <int R, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
-                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf) {
+                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf,
+                     double* __restrict__ grad_partials) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
+  __shared__ double sgrad[kMaxPassGrads];   // this CTA's gradient terms (adjoint passes)
   __shared__ volatile int abort_flag;
 
   // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
@@ -518,6 +576,7 @@ __global__ void __launch_bounds__(NT, MINB)
   const uint32_t tile_elems = 1u << P.M;
   double2* smat = tiles + (size_t)nbuf * tile_elems;
   for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + i];
+  for (uint32_t i = tid; i < P.ngrad; i += NT) sgrad[i] = 0.0;
   if (tid == 0) {
     for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
     abort_flag = 0;
@@ -618,7 +677,7 @@ __global__ void __launch_bounds__(NT, MINB)
     if (!work && first_unwaited == cnt) first_unwaited = i;
     double2* buf = tiles + (size_t)b * tile_elems;
     for (int s = 0; s < P.nstages; ++s) {
-      if (work) run_stage<R>(buf, P, s, smat, tid, NT);
+      if (work) run_stage<R>(buf, P, s, smat, tid, NT, sgrad);
       __syncthreads();
     }
     fence_proxy_async_smem();
@@ -628,6 +687,11 @@ __global__ void __launch_bounds__(NT, MINB)
   // after an abort, let loads that were issued but never consumed land first
   for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
   bulk_wait_all();
+  if (P.ngrad) {   // one column of per-CTA partials per gradient term
+    __syncthreads();
+    for (uint32_t i = tid; i < P.ngrad; i += NT)
+      grad_partials[(size_t)(P.grad_base + i) * gridDim.x + blockIdx.x] = sgrad[i];
+  }
 }
 
 }  // namespace iqb

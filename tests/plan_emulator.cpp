@@ -5,6 +5,7 @@
 // and every operation kind.  It lets the CPU test suite check the scheduler,
 // the descriptor encoding and the tile addressing against the oracle.  It also
 // checks that the box copies of a pass cover every amplitude exactly once.
+#include <algorithm>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,7 @@ struct Emu {
   std::string err;
 
   uint32_t blk = 0;   // current pass's matrix block
+  std::vector<double> grads;   // gradient terms accumulated by OP_GRAD2
   cd mat(uint32_t off, int i) const { return pool[blk + off + i]; }
 
   bool copy_tile(const PassDesc& P, uint64_t t, std::vector<cd>& tile, bool load, std::vector<uint8_t>& seen) {
@@ -161,6 +163,26 @@ struct Emu {
                 }
               }
             break;
+          case OP_GRAD2: {
+            if (od.a != 0) { err = "adjoint step with the select bit outside slot 0"; return false; }
+            if (od.gidx >= grads.size()) grads.resize(od.gidx + 1, 0.0);
+            const int B = od.b;
+            for (int L = 0; L < 8; ++L)
+              for (int v = 0; v < NV; ++v) {
+                if (v & (1 | (1 << B))) continue;
+                const cd p0 = a[L][v], p1 = a[L][v | (1 << B)], l0 = a[L][v | 1], l1 = a[L][v | 1 | (1 << B)];
+                cd t;
+                if (od.perm == 0) t = std::conj(l0) * p1 + std::conj(l1) * p0;
+                else if (od.perm == 1) t = std::conj(l0) * (cd(0, -1) * p1) + std::conj(l1) * (cd(0, 1) * p0);
+                else t = std::conj(l0) * p0 - std::conj(l1) * p1;
+                grads[od.gidx] += t.imag();
+                a[L][v] = mat(od.mat, 0) * p0 + mat(od.mat, 1) * p1;
+                a[L][v | (1 << B)] = mat(od.mat, 2) * p0 + mat(od.mat, 3) * p1;
+                a[L][v | 1] = mat(od.mat, 0) * l0 + mat(od.mat, 1) * l1;
+                a[L][v | 1 | (1 << B)] = mat(od.mat, 2) * l0 + mat(od.mat, 3) * l1;
+              }
+            break;
+          }
           case OP_DKR: {
             const int k = od.k, D = 1 << k;
             if (o != sd.op1 - 1) { err = "dense block is not the last operation of its stage"; return false; }
@@ -187,7 +209,150 @@ struct Emu {
   }
 };
 
+// plan `ops` (optionally fused) and run every pass on `state`
+int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stages, double budget, int fuse,
+             int* npasses, int* ops_per_pass, char* errbuf, int errlen) {
+  if (fuse) {
+    std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(e.pool.data()),
+                           reinterpret_cast<const cplx64*>(e.pool.data()) + e.pool.size());
+    ops = fuse_two_qubit_blocks(ops, cp);
+    e.pool.assign(reinterpret_cast<const cd*>(cp.data()), reinterpret_cast<const cd*>(cp.data()) + cp.size());
+  }
+  SchedParams p{};
+  p.nbits = e.nbits;
+  p.M = M;
+  p.c = c;
+  p.R = R;
+  p.max_stages = max_stages;
+  p.budget = budget;
+  std::vector<PassPlan> plans;
+  std::string err;
+  if (plan_passes(p, ops, plans, err) < 0) {
+    snprintf(errbuf, errlen, "plan: %s", err.c_str());
+    return -1;
+  }
+  if (npasses) *npasses = (int)plans.size();
+  std::vector<cplx64> packed;
+  pack_pass_matrices(plans, reinterpret_cast<const cplx64*>(e.pool.data()), packed);
+  e.pool.assign(reinterpret_cast<const cd*>(packed.data()), reinterpret_cast<const cd*>(packed.data()) + packed.size());
+  for (size_t pi = 0; pi < plans.size(); ++pi) {
+    const PassDesc& P = plans[pi].desc;
+    e.blk = P.mat_base;
+    if (ops_per_pass) ops_per_pass[pi] = plans[pi].nsrc;
+    if (P.mat_elems > (uint32_t)kSmemMatElems) {
+      snprintf(errbuf, errlen, "pass %zu: matrix block exceeds shared memory", pi);
+      return -1;
+    }
+    std::vector<cd> tile((size_t)1 << P.M);
+    std::vector<uint8_t> seen((size_t)1 << e.nbits, 0);
+    for (uint64_t t = 0; t < P.ntiles; ++t) {
+      if (!e.copy_tile(P, t, tile, true, seen)) break;
+      for (int st = 0; st < P.nstages && e.err.empty(); ++st) e.run_stage(P, st, tile);
+      if (!e.err.empty()) break;
+      if (!e.copy_tile(P, t, tile, false, seen)) break;
+    }
+    if (e.err.empty())
+      for (size_t i = 0; i < seen.size(); ++i)
+        if (!seen[i]) { e.err = "amplitude not covered by a pass"; break; }
+    if (!e.err.empty()) {
+      snprintf(errbuf, errlen, "pass %zu: %s", pi, e.err.c_str());
+      return -1;
+    }
+  }
+  return 0;
+}
+
 }  // namespace
+
+// Adjoint gradient of <psi|H|psi> for an ansatz, run through the planned
+// passes exactly as the GPU path does (forward on psi, lambda = H psi, joint
+// array, backward sweep with adjoint steps).  H = sum_t coeffs[t] paulis[t]
+// (n characters per term, character q acting on qubit q).
+extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
+                           const double* params, int nterms, const double* coeffs, const char* paulis, int M, int c,
+                           int max_stages, double budget, double* energy, double* grad, int nparams, char* errbuf,
+                           int errlen) {
+  std::vector<AnsatzOp> ops(nops);
+  for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
+  std::string err;
+  if (ansatz_check(n, ops, err) < 0) {
+    snprintf(errbuf, errlen, "%s", err.c_str());
+    return -1;
+  }
+  // forward
+  Emu f;
+  f.nbits = n;
+  std::vector<cd> psi((size_t)1 << n, 0.0);
+  psi[0] = 1.0;
+  f.state = psi.data();
+  std::vector<SchedOp> fw;
+  std::vector<cplx64> pool;
+  ansatz_forward(n, ops, params, fw, pool);
+  f.pool.assign(reinterpret_cast<const cd*>(pool.data()), reinterpret_cast<const cd*>(pool.data()) + pool.size());
+  if (n >= 7) {
+    if (run_plan(f, fw, M, c, 4, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+  } else {   // the runtime's one-operation kernel: dense matrix, LSB-first qubit list
+    for (const SchedOp& o : fw) {
+      const int d = 1 << o.k;
+      for (uint64_t base = 0; base < (1ULL << n); ++base) {
+        bool lead = true;
+        for (int j = 0; j < o.k; ++j) lead &= !((base >> o.q[j]) & 1);
+        if (!lead) continue;
+        std::vector<uint64_t> idx(d);
+        std::vector<cd> x(d);
+        for (int v = 0; v < d; ++v) {
+          idx[v] = base;
+          for (int j = 0; j < o.k; ++j)
+            if ((v >> j) & 1) idx[v] |= 1ULL << o.q[j];
+          x[v] = psi[idx[v]];
+        }
+        for (int r = 0; r < d; ++r) {
+          cd acc = 0.0;
+          for (int cc = 0; cc < d; ++cc) acc += f.pool[o.dense + r * d + cc] * x[cc];
+          psi[idx[r]] = acc;
+        }
+      }
+    }
+  }
+  // lambda = H psi and the energy
+  const uint64_t dim = 1ULL << n;
+  std::vector<cd> lam(dim, 0.0);
+  for (int t = 0; t < nterms; ++t) {
+    uint64_t xm = 0, zm = 0;
+    int ny = 0;
+    for (int q = 0; q < n; ++q) {
+      const char ch = paulis[t * n + q];
+      if (ch == 'X') xm |= 1ULL << q;
+      else if (ch == 'Y') { xm |= 1ULL << q; zm |= 1ULL << q; ++ny; }
+      else if (ch == 'Z') zm |= 1ULL << q;
+    }
+    const cd ip[4] = {cd(1, 0), cd(0, 1), cd(-1, 0), cd(0, -1)};
+    for (uint64_t j = 0; j < dim; ++j) {
+      const uint64_t i = j ^ xm;
+      const double sg = (__builtin_popcountll(i & zm) & 1) ? -1.0 : 1.0;
+      lam[j] += coeffs[t] * ip[ny & 3] * sg * psi[i];
+    }
+  }
+  cd e = 0.0;
+  for (uint64_t x = 0; x < dim; ++x) e += std::conj(psi[x]) * lam[x];
+  *energy = e.real();
+  // backward on the joint array
+  Emu b;
+  b.nbits = std::max(n + 1, 7);   // small circuits: zero-padded high bits the gates never touch
+  std::vector<cd> joint((size_t)1 << b.nbits, 0.0);
+  for (uint64_t x = 0; x < dim; ++x) { joint[2 * x] = psi[x]; joint[2 * x + 1] = lam[x]; }
+  b.state = joint.data();
+  std::vector<SchedOp> bw;
+  std::vector<cplx64> bpool;
+  std::vector<int> gp;
+  ansatz_backward(n, ops, params, bw, bpool, gp);
+  b.pool.assign(reinterpret_cast<const cd*>(bpool.data()), reinterpret_cast<const cd*>(bpool.data()) + bpool.size());
+  b.grads.assign(gp.size(), 0.0);
+  if (run_plan(b, bw, M, c, 4, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+  for (int p = 0; p < nparams; ++p) grad[p] = 0.0;
+  for (size_t t = 0; t < gp.size(); ++t) grad[gp[t]] += b.grads[t];
+  return 0;
+}
 
 extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double budget, int fuse, int nops,
                          const int* ks, const int* qs, const double* mats, const long long* mat_off,

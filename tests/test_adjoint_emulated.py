@@ -1,0 +1,69 @@
+"""CPU check of the adjoint-gradient pipeline: the op lists built by
+iq_sched.cpp (forward, lambda = H psi, backward sweep of adjoint steps on the
+joint psi/lambda array) run through the planned passes with the kernel's
+semantics (tests/plan_emulator.cpp), against parameter-shift and finite
+differences of oracle energies."""
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from invariantq_b200.circuits import tfim_terms
+from tests import adjoint_ref as ar
+
+REPO = Path(__file__).resolve().parent.parent
+
+
+@pytest.fixture(scope="session")
+def emu(tmp_path_factory):
+    out = tmp_path_factory.mktemp("emuadj") / "libplanemu.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out),
+                    str(REPO / "tests" / "plan_emulator.cpp"),
+                    str(REPO / "invariantq_b200" / "csrc" / "iq_sched.cpp")], check=True)
+    return ctypes.CDLL(str(out))
+
+
+def emu_grad(emu, n, ops, theta, coeffs, paulis, M=11, c=5, stages=8, budget=80.0):
+    k = np.array([o[0] for o in ops], np.int32)
+    q0 = np.array([o[1] for o in ops], np.int32)
+    q1 = np.array([o[2] for o in ops], np.int32)
+    pi = np.array([o[3] for o in ops], np.int32)
+    th = np.ascontiguousarray(theta, np.float64)
+    co = np.ascontiguousarray(coeffs, np.float64)
+    ps = "".join(paulis).encode()
+    e = ctypes.c_double()
+    g = np.zeros(len(theta))
+    err = ctypes.create_string_buffer(256)
+    P = ctypes.c_void_p
+    rc = emu.emu_adjoint(n, len(ops), P(k.ctypes.data), P(q0.ctypes.data), P(q1.ctypes.data), P(pi.ctypes.data),
+                         P(th.ctypes.data), len(coeffs), P(co.ctypes.data), ps, M, c, stages, ctypes.c_double(budget),
+                         ctypes.byref(e), P(g.ctypes.data), len(theta), err, 256)
+    assert rc == 0, err.value
+    return e.value, g
+
+
+@pytest.mark.parametrize("n,layers,seed", [(6, 2, 0), (8, 3, 1), (9, 2, 2)])
+def test_tfim_ansatz_gradient(port, emu, n, layers, seed):
+    rng = np.random.default_rng(seed)
+    ops = ar.tfim_ops(n, layers)
+    theta = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
+    coeffs, paulis = tfim_terms(n, 0.7)
+    e, g = emu_grad(emu, n, ops, theta, coeffs, paulis)
+    assert abs(e - ar.energy(port, n, ops, theta, coeffs, paulis)) < 1e-12
+    assert np.max(np.abs(g - ar.param_shift(port, n, ops, theta, coeffs, paulis))) < 1e-10
+    assert np.max(np.abs(g - ar.finite_diff(port, n, ops, theta, coeffs, paulis))) < 1e-7
+
+
+@pytest.mark.parametrize("n,ngates,seed", [(5, 40, 3), (7, 60, 4), (8, 80, 5)])
+def test_mixed_gates_gradient(port, emu, n, ngates, seed):
+    rng = np.random.default_rng(seed)
+    ops = ar.random_ansatz(rng, n, ngates)
+    theta = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
+    # a random Pauli observable with X, Y and Z terms
+    paulis = ["".join(rng.choice(list("IXYZ"), n)) for _ in range(6)]
+    coeffs = rng.normal(size=6)
+    e, g = emu_grad(emu, n, ops, theta, coeffs, paulis, budget=60.0, stages=4)
+    assert abs(e - ar.energy(port, n, ops, theta, coeffs, paulis)) < 1e-12
+    assert np.max(np.abs(g - ar.param_shift(port, n, ops, theta, coeffs, paulis))) < 1e-10

@@ -1,0 +1,135 @@
+"""GPU adjoint gradients against parameter-shift and central finite differences
+of oracle energies, the GPU parameter-shift path, the batch executor and the
+autograd wrapper.
+
+Tolerances: energy 1e-12; gradient vs parameter-shift 1e-9 (both exact
+methods; they agree to ~1e-15 in practice); gradient vs central differences
+with step 1e-6: 5e-9, because the difference quotient itself carries a
+rounding error of about eps * |E| / h ~ 1e-9."""
+import numpy as np
+import pytest
+
+from invariantq_b200.circuits import tfim_terms
+from tests import adjoint_ref as ar
+
+pytestmark = pytest.mark.gpu
+PS_TOL = 1e-9
+FD_TOL = 5e-9
+
+
+@pytest.fixture(scope="module")
+def G():
+    from invariantq_b200 import gradients
+    return gradients
+
+
+def ansatz_of(G, n, ops):
+    return G.Ansatz(n, [(k, (a,) if b < 0 else (a, b), p) for k, a, b, p in ops])
+
+
+@pytest.mark.parametrize("n,layers,seed", [(3, 2, 0), (6, 2, 1), (8, 3, 2), (11, 2, 3)])
+def test_tfim_gradient_vs_oracle(G, port, n, layers, seed):
+    rng = np.random.default_rng(seed)
+    ops = ar.tfim_ops(n, layers)
+    th = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
+    coeffs, paulis = tfim_terms(n, 1.0)
+    e, g = G.adjoint_gradient(ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis), th)
+    assert abs(e - ar.energy(port, n, ops, th, coeffs, paulis)) < 1e-12
+    assert np.max(np.abs(g - ar.param_shift(port, n, ops, th, coeffs, paulis))) < PS_TOL
+    assert np.max(np.abs(g - ar.finite_diff(port, n, ops, th, coeffs, paulis))) < FD_TOL
+
+
+@pytest.mark.parametrize("n,ngates,seed", [(2, 20, 4), (5, 50, 5), (7, 80, 6), (9, 120, 7)])
+def test_mixed_gates_gradient_vs_oracle(G, port, n, ngates, seed):
+    """RX/RY/RZ/U3/P rotations among H/SX/CZ/CX, and Y terms in H."""
+    rng = np.random.default_rng(seed)
+    ops = ar.random_ansatz(rng, n, ngates)
+    th = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
+    paulis = ["".join(rng.choice(list("IXYZ"), n)) for _ in range(6)]
+    coeffs = rng.normal(size=6)
+    e, g = G.adjoint_gradient(ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis), th)
+    assert abs(e - ar.energy(port, n, ops, th, coeffs, paulis)) < 1e-12
+    assert np.max(np.abs(g - ar.param_shift(port, n, ops, th, coeffs, paulis))) < PS_TOL
+
+
+def test_gpu_parameter_shift_matches_oracle(G, port):
+    n, ops = 7, ar.tfim_ops(7, 2)
+    th = np.random.default_rng(8).uniform(0, 2 * np.pi, ar.n_params(ops))
+    coeffs, paulis = tfim_terms(n, 0.7)
+    a, h = ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis)
+    assert np.max(np.abs(G.parameter_shift_gradient(a, h, th) - ar.param_shift(port, n, ops, th, coeffs, paulis))) < 1e-12
+    assert abs(G.ansatz_energies(a, h, th)[0] - ar.energy(port, n, ops, th, coeffs, paulis)) < 1e-12
+
+
+@pytest.mark.parametrize("n,layers", [(16, 2), (20, 1)])
+def test_large_gradient_vs_gpu_parameter_shift(G, n, layers):
+    """Multi-tile circuits: adjoint vs the plain GPU path's parameter shift."""
+    a, h = G.Ansatz.hardware_efficient(n, layers), G.PauliHamiltonian.tfim(n, 1.0)
+    th = np.random.default_rng(n).uniform(0, 2 * np.pi, a.num_params)
+    e, g = G.adjoint_gradient(a, h, th)
+    assert abs(e - G.ansatz_energies(a, h, th)[0]) < 1e-12
+    assert np.max(np.abs(g - G.parameter_shift_gradient(a, h, th))) < PS_TOL
+
+
+def test_batch_matches_single_jobs(G):
+    """Uneven circuits and several parameter sets on several streams give the
+    same numbers as one job at a time (same plans, fixed reduction order)."""
+    rng = np.random.default_rng(9)
+    jobs = []
+    for n, L in [(4, 2), (10, 3), (13, 2), (7, 4), (12, 1)]:
+        a, h = G.Ansatz.hardware_efficient(n, L), G.PauliHamiltonian.tfim(n, 1.0)
+        jobs.append((a, h, rng.uniform(0, 2 * np.pi, (3, a.num_params))))
+    out = G.adjoint_gradient_batch(jobs, num_streams=4)
+    st = G.adjoint_stats()
+    assert st["jobs"] == 15 and st["streams"] == 4
+    for (a, h, P), (e, g) in zip(jobs, out):
+        for s in range(P.shape[0]):
+            e1, g1 = G.adjoint_gradient(a, h, P[s])
+            assert e[s] == e1
+            assert np.array_equal(g[s], g1)
+            assert np.max(np.abs(g[s] - G.parameter_shift_gradient(a, h, P[s]))) < PS_TOL
+
+
+def test_structure_change_across_sets_is_replanned(G, port):
+    """An angle of 0 turns a fused block monomial: that set gets its own plan."""
+    n, ops = 8, ar.tfim_ops(8, 2)
+    coeffs, paulis = tfim_terms(n, 1.0)
+    a, h = ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis)
+    rng = np.random.default_rng(10)
+    P = rng.uniform(0, 2 * np.pi, (2, a.num_params))
+    P[1, :n] = 0.0
+    (e, g), = G.adjoint_gradient_batch([(a, h, P)], num_streams=1)
+    for s in range(2):
+        assert abs(e[s] - ar.energy(port, n, ops, P[s], coeffs, paulis)) < 1e-12
+        assert np.max(np.abs(g[s] - ar.param_shift(port, n, ops, P[s], coeffs, paulis))) < PS_TOL
+
+
+def test_autograd_function(G):
+    import torch
+    n = 9
+    a, h = G.Ansatz.hardware_efficient(n, 2), G.PauliHamiltonian.tfim(n, 1.0)
+    th = torch.tensor(np.random.default_rng(11).uniform(0, 2 * np.pi, a.num_params), requires_grad=True)
+    e = G.expectation(th, a, h)
+    (2.0 * e).backward()
+    e_ref, g_ref = G.adjoint_gradient(a, h, th.detach().numpy())
+    assert abs(e.item() - e_ref) < 1e-14
+    assert torch.allclose(th.grad, torch.from_numpy(2.0 * g_ref), atol=0, rtol=0)
+    P = torch.tensor(np.random.default_rng(12).uniform(0, 2 * np.pi, (3, a.num_params)), requires_grad=True)
+    E = G.expectation(P, a, h)
+    w = torch.tensor([1.0, -2.0, 0.5], dtype=torch.float64)
+    (E * w).sum().backward()
+    for s in range(3):
+        _, gs = G.adjoint_gradient(a, h, P[s].detach().numpy())
+        assert torch.allclose(P.grad[s], w[s] * torch.from_numpy(gs), atol=1e-15, rtol=0)
+
+
+def test_invalid_inputs_raise(G):
+    a = G.Ansatz(3, [("rx", (0,), 0), ("cx", (1, 2), -1)])
+    with pytest.raises(ValueError):
+        G.adjoint_gradient(G.Ansatz(3, [("cz", (1, 1), -1)]), G.PauliHamiltonian.tfim(3), np.zeros(0))
+    with pytest.raises(ValueError):
+        G.adjoint_gradient(a, G.PauliHamiltonian(3, [1.0], ["XQZ"]), np.zeros(1))
+    with pytest.raises(ValueError):
+        G.adjoint_gradient(G.Ansatz(3, [("rx", (5,), 0)]), G.PauliHamiltonian.tfim(3), np.zeros(1))
+    e, g = G.adjoint_gradient(a, G.PauliHamiltonian(3, [0.5], ["IIZ"]), np.array([0.3]))
+    assert abs(e - 0.5) < 1e-15 and abs(g[0]) < 1e-15
