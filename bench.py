@@ -63,6 +63,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-gates", type=int, default=4, help="gates per step of the reference arm")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the batched adjoint-gradient measurement")
+    ap.add_argument("--adjoint-circuits", type=int, default=256)
+    ap.add_argument("--adjoint-sets", type=int, default=16)
+    ap.add_argument("--adjoint-steps", type=int, default=2)
+    ap.add_argument("--adjoint-streams", type=int, default=0)
+    ap.add_argument("--ps-stride", type=int, default=16,
+                    help="parameter-shift baseline on every k-th circuit (one parameter set each)")
     return ap.parse_args()
 
 
@@ -85,16 +92,16 @@ def measured_peaks():
 
 
 def traffic_record(n):
-    """DRAM bytes per tile-pass launch from the committed ncu summary, if any."""
-    p = REPO / "profiles" / "tile_pass_traffic.json"
+    """DRAM bytes per tile-pass launch from the committed ncu summary
+    (profiles/tile_pass_traffic.txt: `qubits Q` and `bytes_per_launch B`),
+    scaled to n qubits by the amplitudes per launch."""
+    p = REPO / "profiles" / "tile_pass_traffic.txt"
     if not p.exists():
         return None
     try:
-        d = json.loads(p.read_text())
-        if int(d.get("qubits", -1)) == n:
-            return float(d["bytes_per_launch"])
-        # traffic grows with the array: scale by amplitudes per launch
-        return float(d["bytes_per_launch"]) * (2.0 ** (n - int(d["qubits"])))
+        kv = dict(line.split()[:2] for line in p.read_text().splitlines() if line.strip() and not line.startswith("#"))
+        q, b = int(kv["qubits"]), float(kv["bytes_per_launch"])
+        return b * (2.0 ** (n - q))
     except Exception:
         return None
 
@@ -240,6 +247,73 @@ def reference_arm(args, rank):
     print(json.dumps(out))
 
 
+# ------------------------------------------------------- batched adjoint gradients
+
+def gradient_jobs(ncirc, nsets, seed=1234):
+    """256 circuits with n ~ U{10..22}, L ~ U{4..12}; per layer RY and RZ on every
+    qubit then a CZ ring; 16 parameter sets of angles ~ U[0, 2 pi); H = TFIM,
+    h = 1.0, open boundary."""
+    from invariantq_b200.gradients import Ansatz, PauliHamiltonian
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(ncirc):
+        n = int(rng.integers(10, 23))
+        L = int(rng.integers(4, 13))
+        a = Ansatz.hardware_efficient(n, L)
+        jobs.append((a, PauliHamiltonian.tfim(n, 1.0), rng.uniform(0, 2 * np.pi, (nsets, a.num_params))))
+    return jobs
+
+
+def adjoint_section(args, rank, world):
+    """grads/s of the batch API on this rank's share of the circuits (weak:
+    circuits split across ranks, no collective on the data path) and the plain
+    one-circuit-at-a-time parameter-shift path on a sample of the same circuits."""
+    import torch
+    from invariantq_b200.gradients import adjoint_gradient_batch, adjoint_stats, parameter_shift_gradient
+    jobs = gradient_jobs(args.adjoint_circuits, args.adjoint_sets)
+    mine = jobs[rank::world]
+    grads = sum(P.shape[0] for _, _, P in mine)
+    partials = sum(P.shape[0] * P.shape[1] for _, _, P in mine)
+    adjoint_gradient_batch(mine, args.adjoint_streams)            # warm-up (allocations, first plans)
+    times = []
+    for _ in range(max(args.adjoint_steps, 1)):
+        t0 = time.perf_counter()
+        out = adjoint_gradient_batch(mine, args.adjoint_streams)
+        times.append(time.perf_counter() - t0)
+    st = adjoint_stats()
+    t = float(np.median(times))
+    if world > 1:
+        x = torch.tensor([t], dtype=torch.float64, device=f"cuda:{int(os.environ.get('LOCAL_RANK', 0))}")
+        torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
+        t = float(x.item())
+    # parameter-shift baseline on every k-th circuit of this rank (first parameter set)
+    ps_t, ps_n, err = 0.0, 0, 0.0
+    for i in range(0, len(mine), max(args.ps_stride, 1)):
+        a, h, P = mine[i]
+        t0 = time.perf_counter()
+        g = parameter_shift_gradient(a, h, P[0])
+        ps_t += time.perf_counter() - t0
+        ps_n += 1
+        err = max(err, float(np.max(np.abs(g - out[i][1][0]))))
+    ps_rate = ps_n / ps_t
+    ns = [a.num_qubits for a, _, _ in mine]
+    return {
+        "metric": "batched adjoint grads/s", "value": round(world * grads / t, 2), "unit": "gradients/s",
+        "partials_per_s": round(world * partials / t, 1), "batch_s": round(t, 4), "steps": len(times),
+        "warmup": 1, "gradients": world * grads, "streams": int(st["streams"]),
+        "passes": {"forward": int(st["forward_passes"]), "backward": int(st["backward_passes"])},
+        "achieved_gbs": round(st["bytes"] / t / 1e9, 1), "host_prep_ms": round(st["host_ms"], 1),
+        "workload": f"{args.adjoint_circuits} circuits n~U{{10..22}} (here {min(ns)}..{max(ns)}), L~U{{4..12}}, "
+                    f"RY+RZ per qubit + CZ ring per layer, {args.adjoint_sets} parameter sets each, TFIM h=1.0, "
+                    "complex128; timed through iq_adjoint_gradient_batch (host parameters in, host gradients out)",
+        "param_shift": {"grads_per_s": round(world * ps_rate, 3), "sample": f"{ps_n} circuits (every "
+                        f"{args.ps_stride}th, first parameter set), 2P plain forward simulations + energy each",
+                        "seconds": round(ps_t, 2)},
+        "speedup_vs_param_shift": round((grads / t) / ps_rate, 1),
+        "max_abs_diff_vs_param_shift": err,
+    }
+
+
 # ---------------------------------------------------------------- our arm
 
 def our_arm(args, rank, world, local_rank):
@@ -328,6 +402,7 @@ def our_arm(args, rank, world, local_rank):
                "ms_per_step": round(e2e_ms, 3)}
         assert np.all(np.abs(z) <= 1.0 + 1e-9)
 
+    adj = adjoint_section(args, rank, world) if not args.no_adjoint else None
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
@@ -360,6 +435,8 @@ def our_arm(args, rank, world, local_rank):
         "e2e": e2e,
         "clocks": clk,
     }
+    if adj is not None:
+        out["adjoint"] = adj
     if world == 1 and not args.no_cpu_baseline:
         gbs, done, nq, kind, threads, dt = cpu_reference_run(gates, n, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": kind,

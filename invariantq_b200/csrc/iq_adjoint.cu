@@ -69,6 +69,7 @@ struct Cfg {
     c.sp.R = 4;
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
     c.sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
+    c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
     c.tl.nbuf = env_int("IQ_NBUF", 3);
     c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
     c.tl.consumers = 128;
@@ -481,7 +482,9 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set, bool want_
   // staging slot: wait for the job that used it last
   const int k = w.slot;
   w.slot ^= 1;
+  const auto tw = std::chrono::steady_clock::now();
   if (!finish(w, k, err)) return false;
+  const auto tw1 = std::chrono::steady_clock::now();
   const size_t nf = fw->gather.size(), nb = want_grad ? bw->gather.size() : 0;
   if (!w.hmats[k].ensure(nf + nb, err) || !w.hout[k].ensure(1 + (size_t)ngrads, err) || !w.hstat[k].ensure(1, err))
     return false;
@@ -513,8 +516,9 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set, bool want_
   if (!cuda_ok(cudaMemcpyAsync(dm, hm, (nf + nb) * sizeof(double2), cudaMemcpyHostToDevice, w.stream), "H2D matrices",
                err))
     return false;
-  st.host_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0)
-                    .count();
+  st.host_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                     (std::chrono::steady_clock::now() - t0) - (tw1 - tw))
+                     .count();
 
   // forward from |0>
   const uint64_t dim = 1ULL << c.n;

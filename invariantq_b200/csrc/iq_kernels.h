@@ -28,7 +28,9 @@ int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d,
 // grad_partials: [gradient term][CTA] partial sums of the pass's OP_GRAD2 terms (or null)
 cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
                              const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials = nullptr);
-size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems);
+// dynamic shared memory of a pass: tile buffers, matrix block, gradient accumulators
+size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems, uint32_t ngrad);
+constexpr int kTileThreads = 128;   // threads per tile-pass CTA (every instantiation)
 // one launcher per kernel instantiation (iq_tile_r4.cu, iq_tile_r5.cu)
 cudaError_t launch_tile_r4(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
                            unsigned grid, size_t smem, cudaStream_t st, double* grad_partials);

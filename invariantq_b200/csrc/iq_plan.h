@@ -48,7 +48,9 @@ enum OpKind : uint8_t {
   OP_M2R = 7,   // monomial 4x4, register slots a (bit 0) and b (bit 1)
   OP_GRAD2 = 8, // adjoint step on slots a (psi/lambda select bit) and b (qubit bit): add
                 // Im<lambda|P|psi> (P = X, Y, Z for `perm` = 0, 1, 2) to gradient term
-                // `gidx`, then apply the 2x2 matrix at `mat` to the qubit for both halves
+                // `gidx`, then apply the 2x2 matrix at `mat` to the qubit for both halves; the
+                // matrix is the inverse rotation exp(+i t P / 2) and is read through its
+                // structure (entries 0, 1, 3)
 };
 
 // flags
@@ -108,6 +110,7 @@ struct SchedParams {
   int R;                 // register slots per thread (4 or 5)
   int max_stages;        // stages per pass (each costs one shared-memory round trip)
   double budget;         // max arithmetic cost per pass (real FMAs per amplitude)
+  double grad_cost = 6.0;    // cost of an adjoint step: a structured rotation on both halves (4) plus its products
 };
 
 // A planned pass.  desc.ops[].mat are offsets into the caller's op matrix pool

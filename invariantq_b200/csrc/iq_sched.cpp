@@ -26,8 +26,8 @@ int op_mat_elems(const SchedOp& op) {
   return op.mono ? (1 << op.k) : (1 << (2 * op.k));
 }
 
-double op_cost(const SchedOp& op) {
-  if (op.grad) return 24.0;   // 2x2 on both halves plus the gradient products
+double op_cost(const SchedOp& op, double grad_cost) {
+  if (op.grad) return grad_cost;   // 2x2 on both halves plus the gradient products
   if (op.mono) return op.unit ? 0.25 : 4.0;
   return 4.0 * double(1u << op.k);
 }
@@ -275,7 +275,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         for (auto it = ready.begin(); it != ready.end();) {
           const int i = *it;
           const SchedOp& o = ops[i];
-          const double oc = op_cost(o);
+          const double oc = op_cost(o, p.grad_cost);
           if ((opmask(o) & ~local) == 0 && (int)taken.size() < kMaxPassOps &&
               mat_elems + op_mat_elems(o) <= kSmemMatElems && (taken.empty() || cost + oc <= p.budget) &&
               (!o.grad || ngrad < kMaxPassGrads) && pb.place(i, o)) {
@@ -295,7 +295,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
       int best = -1, bestmiss = 0;
       for (int i : ready) {
         const int miss = __builtin_popcountll(opmask(ops[i]) & ~local);
-        if (miss > 0 && miss <= free_slots && (taken.empty() || cost + op_cost(ops[i]) <= p.budget)) {
+        if (miss > 0 && miss <= free_slots && (taken.empty() || cost + op_cost(ops[i], p.grad_cost) <= p.budget)) {
           best = i;
           bestmiss = miss;
           break;

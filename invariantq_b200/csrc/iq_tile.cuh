@@ -18,9 +18,34 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "iq_kernels.h"
 
 namespace iqb {
+
+// Raise a kernel's dynamic shared-memory limit to everything the device allows
+// beside the kernel's static shared memory, once per device.  Setting it per
+// launch to the launch's own size races between host threads: another thread's
+// smaller setting can land between this thread's setting and its launch.
+// Occupancy still follows each launch's actual dynamic size.
+template <class K>
+inline cudaError_t allow_full_dynamic_smem(K kern, std::atomic<uint64_t>& done) {
+  int dev = 0;
+  cudaError_t r = cudaGetDevice(&dev);
+  if (r != cudaSuccess) return r;
+  const uint64_t bit = 1ULL << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+  int optin = 0;
+  r = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (r != cudaSuccess) return r;
+  cudaFuncAttributes fa{};
+  r = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kern));
+  if (r != cudaSuccess) return r;
+  r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  if (r == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+  return r;
+}
 
 // ------------------------------------------------------------------ helpers
 
@@ -363,11 +388,31 @@ __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 <
 
 // Adjoint step on slot 0 (psi / lambda select bit) and slot B (the qubit):
 // returns this thread's share of Im<lambda| P |psi> for generator P (GEN 0 = X,
-// 1 = Y, 2 = Z), then applies the 2x2 matrix (the inverse gate) to the qubit
-// in both halves.  Inputs are read before outputs are written (in-place safe).
+// 1 = Y, 2 = Z), then un-applies the rotation exp(-i t P / 2) on the qubit in
+// both halves.  m is the inverse rotation, used through its structure:
+// GEN 0: [[c, i s], [i s, c]]; GEN 1: [[c, s], [-s, c]] (real);
+// GEN 2: diag(e^{i t/2}, e^{-i t/2}).  Inputs are read before outputs are
+// written (in-place safe).
+template <int GEN>
+__device__ __forceinline__ void unrotate(double2 x0, double2 x1, double2& y0, double2& y1, double2 u0, double2 u1,
+                                         double2 u3) {
+  if (GEN == 0) {         // y0 = c x0 + i s x1, y1 = i s x0 + c x1
+    const double c = u0.x, sn = u1.y;
+    y0 = make_double2(fma(c, x0.x, -sn * x1.y), fma(c, x0.y, sn * x1.x));
+    y1 = make_double2(fma(c, x1.x, -sn * x0.y), fma(c, x1.y, sn * x0.x));
+  } else if (GEN == 1) {  // y0 = c x0 + s x1, y1 = c x1 - s x0
+    const double c = u0.x, sn = u1.x;
+    y0 = make_double2(fma(c, x0.x, sn * x1.x), fma(c, x0.y, sn * x1.y));
+    y1 = make_double2(fma(c, x1.x, -sn * x0.x), fma(c, x1.y, -sn * x0.y));
+  } else {                // diagonal phases
+    y0 = cmul(u0, x0);
+    y1 = cmul(u3, x1);
+  }
+}
+
 template <int R, int B, int GEN>
 __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
-  const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
+  const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u3 = ld_mat(m, 3);
   double acc = 0.0;
 #pragma unroll
   for (int v = 0; v < (1 << R); ++v) {
@@ -380,10 +425,8 @@ __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)
     } else {                // Z: (P psi)_0 = psi_0, (P psi)_1 = -psi_1
       acc += (l0.x * p0.y - l0.y * p0.x) - (l1.x * p1.y - l1.y * p1.x);
     }
-    d[v] = cfma(cmul(u0, p0), u1, p1);
-    d[v | (1 << B)] = cfma(cmul(u2, p0), u3, p1);
-    d[v | 1] = cfma(cmul(u0, l0), u1, l1);
-    d[v | 1 | (1 << B)] = cfma(cmul(u2, l0), u3, l1);
+    unrotate<GEN>(p0, p1, d[v], d[v | (1 << B)], u0, u1, u3);
+    unrotate<GEN>(l0, l1, d[v | 1], d[v | 1 | (1 << B)], u0, u1, u3);
   }
   return acc;
 }
@@ -461,12 +504,14 @@ __device__ __forceinline__ double disp_grad2_b(int sb, const double2 (&s)[1 << R
 }
 
 // the octet's eight lanes hold the same registers of eight tile rows: sum
-// their shares, and one lane adds it to the CTA's accumulator in shared memory
+// their shares, and the octet's lane 0 -- the only writer of its row of
+// accumulators -- adds it there.  Tiles reach a CTA, and tile rows reach an
+// octet, in a fixed order, so the sums are reproducible bit for bit.
 __device__ __forceinline__ void grad_accumulate(double acc, double* slot, int lane8, unsigned omask) {
   acc += __shfl_xor_sync(omask, acc, 1, 8);
   acc += __shfl_xor_sync(omask, acc, 2, 8);
   acc += __shfl_xor_sync(omask, acc, 4, 8);
-  if (lane8 == 0) atomicAdd(slot, acc);
+  if (lane8 == 0) *slot += acc;
 }
 
 // Apply one operation from s to d; returns true when it wrote the tile itself.
@@ -503,9 +548,10 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
 // lives in shared-memory slot swz(j); every offset below is kept swizzled.
 template <int R>
 __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int s, const double2* mats,
-                                          int ctid, int ncons, double* sgrad) {
+                                          int ctid, int ncons, double* gslots) {
   constexpr int NV = 1 << R;
   const StageDesc& sd = P.st[s];
+  double* sgrad = gslots + (ctid >> 3) * P.ngrad;   // this octet's row of gradient accumulators
   const int lane8 = ctid & 7;
   const unsigned omask = 0xFFu << (ctid & 24);
   const uint32_t laneoff = ((uint32_t)(lane8 & 1) << sd.lane[0]) | ((uint32_t)((lane8 >> 1) & 1) << sd.lane[1]) |
@@ -566,17 +612,18 @@ __global__ void __launch_bounds__(NT, MINB)
                      double* __restrict__ grad_partials) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
-  __shared__ double sgrad[kMaxPassGrads];   // this CTA's gradient terms (adjoint passes)
   __shared__ volatile int abort_flag;
 
   // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
+  // [gradient accumulators: one row of ngrad per octet of threads (adjoint passes)]
   double2* tiles = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const uint32_t tile_elems = 1u << P.M;
   double2* smat = tiles + (size_t)nbuf * tile_elems;
   for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + i];
-  for (uint32_t i = tid; i < P.ngrad; i += NT) sgrad[i] = 0.0;
+  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
+  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
   if (tid == 0) {
     for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
     abort_flag = 0;
@@ -677,7 +724,7 @@ __global__ void __launch_bounds__(NT, MINB)
     if (!work && first_unwaited == cnt) first_unwaited = i;
     double2* buf = tiles + (size_t)b * tile_elems;
     for (int s = 0; s < P.nstages; ++s) {
-      if (work) run_stage<R>(buf, P, s, smat, tid, NT, sgrad);
+      if (work) run_stage<R>(buf, P, s, smat, tid, NT, gslots);
       __syncthreads();
     }
     fence_proxy_async_smem();
@@ -687,10 +734,13 @@ __global__ void __launch_bounds__(NT, MINB)
   // after an abort, let loads that were issued but never consumed land first
   for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
   bulk_wait_all();
-  if (P.ngrad) {   // one column of per-CTA partials per gradient term
+  if (P.ngrad) {   // one column of per-CTA partials per gradient term, octet rows summed in order
     __syncthreads();
-    for (uint32_t i = tid; i < P.ngrad; i += NT)
-      grad_partials[(size_t)(P.grad_base + i) * gridDim.x + blockIdx.x] = sgrad[i];
+    for (uint32_t i = tid; i < P.ngrad; i += NT) {
+      double v = 0.0;
+      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
+      grad_partials[(size_t)(P.grad_base + i) * gridDim.x + blockIdx.x] = v;
+    }
   }
 }
 

@@ -4,8 +4,9 @@ autograd wrapper.
 
 Tolerances: energy 1e-12; gradient vs parameter-shift 1e-9 (both exact
 methods; they agree to ~1e-15 in practice); gradient vs central differences
-with step 1e-6: 5e-9, because the difference quotient itself carries a
-rounding error of about eps * |E| / h ~ 1e-9."""
+with step 1e-6: 1e-9 + 5e-10 * sum|c_t|, because the difference quotient
+itself carries a rounding error of about eps * ||H|| / h (||H|| <= sum|c_t|;
+5.5e-9 observed at 11 qubits, sum|c_t| = 21)."""
 import numpy as np
 import pytest
 
@@ -14,7 +15,10 @@ from tests import adjoint_ref as ar
 
 pytestmark = pytest.mark.gpu
 PS_TOL = 1e-9
-FD_TOL = 5e-9
+
+
+def fd_tol(coeffs):
+    return 1e-9 + 5e-10 * float(np.sum(np.abs(coeffs)))
 
 
 @pytest.fixture(scope="module")
@@ -36,7 +40,7 @@ def test_tfim_gradient_vs_oracle(G, port, n, layers, seed):
     e, g = G.adjoint_gradient(ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis), th)
     assert abs(e - ar.energy(port, n, ops, th, coeffs, paulis)) < 1e-12
     assert np.max(np.abs(g - ar.param_shift(port, n, ops, th, coeffs, paulis))) < PS_TOL
-    assert np.max(np.abs(g - ar.finite_diff(port, n, ops, th, coeffs, paulis))) < FD_TOL
+    assert np.max(np.abs(g - ar.finite_diff(port, n, ops, th, coeffs, paulis))) < fd_tol(coeffs)
 
 
 @pytest.mark.parametrize("n,ngates,seed", [(2, 20, 4), (5, 50, 5), (7, 80, 6), (9, 120, 7)])
