@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--budget", type=float, default=None)
     ap.add_argument("--max-stages", type=int, default=None)
     ap.add_argument("--nbuf", type=int, default=None)
+    ap.add_argument("--reg-slots", type=int, default=None, help="register slots R of the tile kernel (3, 4, 5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -68,6 +69,9 @@ def parse():
     ap.add_argument("--adjoint-sets", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=2)
     ap.add_argument("--adjoint-streams", type=int, default=0)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 20q, fusion-sweep, density-matrix and 30q-adjoint sections")
+    ap.add_argument("--dm-cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ps-stride", type=int, default=16,
                     help="parameter-shift baseline on every k-th circuit (one parameter set each)")
     return ap.parse_args()
@@ -314,6 +318,227 @@ def adjoint_section(args, rank, world):
     }
 
 
+# --------------------------------------------------------------- other configs
+
+def cuda_ms(stream, fn, reps=1):
+    """Device time of fn() on `stream` (CUDA events), averaged over reps."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def brickwall20_section(args):
+    """20-qubit depth-20 brick-wall with every output the workload asks for
+    (statevector, 2^20 probabilities, <Z_i>, 8192 shots) through the C ABI,
+    wall clock per run; beside it the reference core doing the same on the
+    host, and the agreement of the two."""
+    from invariantq_b200.binding import NativeStateVector
+    from invariantq_b200.simulator import apply_gate_matrix
+    from oracle.oracle import RefCore
+    n, depth = 20, 20
+    gates = circuit_gates(n, depth, args.seed)
+    sv = NativeStateVector(n)
+
+    def gpu_run():
+        sv.reset()
+        for qs, U in gates:
+            apply_gate_matrix(sv, qs, U)
+        return sv.get_amplitudes(), sv.get_probabilities(), sv.expval_z_all(), sv.sample(8192, seed=7)
+
+    gpu_run()
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        amps, probs, z, shots = gpu_run()
+        ts.append(time.perf_counter() - t0)
+    sv.close()
+    out = {"workload": f"statevector {n}q brick-wall U3+CX depth {depth} ({len(gates)} gates) + all probabilities, "
+                       "<Z_i> for every qubit, 8192 shots", "gpu_ms": round(1e3 * float(np.median(ts)), 3)}
+    try:
+        core = RefCore()
+    except FileNotFoundError:
+        out["cpu"] = "reference core not built"
+        return out
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    ref = core.sv(n)
+    t0 = time.perf_counter()
+    for qs, U in gates:
+        (ref.apply_1q(qs[0], U) if len(qs) == 1 else ref.apply_2q(qs[0], qs[1], U))
+    ramps = ref.amplitudes()
+    rprobs = ref.probabilities()
+    rz = np.array([ref.expval_pauli("Z", [q]).real for q in range(n)])
+    rshots = ref.sample(8192, 7)
+    cpu_s = time.perf_counter() - t0
+    out.update({"cpu_ms": round(cpu_s * 1e3, 1), "cpu_kind": "reference", "cpu_cores": threads,
+                "speedup_vs_cpu": round(cpu_s * 1e3 / out["gpu_ms"], 1),
+                "max_abs_amp_diff": float(np.max(np.abs(amps - ramps))),
+                "max_abs_prob_diff": float(np.max(np.abs(probs - rprobs))),
+                "max_abs_z_diff": float(np.max(np.abs(z - rz))),
+                "shots_identical_frac": float(np.mean(np.asarray(shots) == np.asarray(rshots)))})
+    return out
+
+
+def fusion_sweep_section(args, sv, n, stream):
+    """The 30-qubit circuit through GateFusionPass at k = 2..5: blocks, tile
+    passes after planning, passes/s and GB/s (2 x 16 B x 2^n per pass)."""
+    from invariantq_b200.circuits import brickwall
+    from invariantq_b200.fusion import GateFusionPass
+    from invariantq_b200.simulator import apply_gate_matrix
+    c = brickwall(n, args.depth, seed=args.seed)
+    out = {}
+    for k in (2, 3, 4, 5):
+        f = GateFusionPass(k).run(c)
+        with sv.record() as rec:
+            for op in f.ops:
+                qs = [f.get_qubit_index(q) for q in op.qubits]
+                if type(op).__name__ == "FusedGateOp":
+                    sv.apply_fused(qs, op.fused_matrix)
+                else:
+                    apply_gate_matrix(sv, qs, op.matrix)
+        prog = rec.program
+
+        def step():
+            sv.reset()
+            prog.run(sv)
+
+        step()
+        sv.sync()
+        ms = cuda_ms(stream, step)
+        sv.sync()
+        out[str(k)] = {"blocks": len(f.ops), "passes": prog.passes, "circuit_ms": round(ms, 2),
+                       "passes_per_s": round(prog.passes / (ms / 1e3), 2),
+                       "GBs": round(prog.passes * pass_bytes(n) / (ms / 1e3) / 1e9, 1)}
+        del prog
+    return out
+
+
+def density_matrix_section(args):
+    """14-qubit noisy brick-wall of depth 12 as a density matrix (4 GiB):
+    depolarizing(1e-3) after every U3, amplitude (2e-3) and phase (1e-3)
+    damping on both qubits after every CX, thermal relaxation (100 us, 80 us,
+    50 ns) on every qubit at each layer end.  Outputs trace, purity,
+    <Z_i Z_i+1>.  GPU: the whole circuit as a recorded program, wall clock of
+    reset + program + trace readback (best of 2 after a warm-up); CPU: the
+    reference core on the first operations of the same circuit."""
+    from invariantq_b200.binding import NativeDensityMatrix
+    from invariantq_b200.channels import build_kraus_channel
+    from invariantq_b200.circuits import noisy_brickwall
+    from oracle.oracle import RefCore
+    n, depth = 14, 12
+    c = noisy_brickwall(n, depth, seed=args.seed)
+    dep = build_kraus_channel("depolarizing", [1e-3])
+    ops = []
+    for op in c.ops:
+        qs = [c.get_qubit_index(q) for q in op.qubits]
+        if type(op).__name__ == "GateOp":
+            if len(qs) == 1:
+                ops += [("u1", qs, op.matrix), ("k1", qs, dep)]
+            else:
+                ops.append(("u2", qs, op.matrix))
+        else:
+            K = build_kraus_channel(op.channel_name, op.params)
+            ops += [("k1", [q], K) for q in qs]
+
+    def apply(target, o):
+        kind, qs, m = o
+        if kind == "u1":
+            target.apply_1q_unitary(qs[0], m)
+        elif kind == "u2":
+            target.apply_2q_unitary(qs[0], qs[1], m)
+        else:
+            target.apply_1q_kraus(qs[0], m)
+
+    dm = NativeDensityMatrix(n)
+    with dm.record() as rec:
+        for o in ops:
+            apply(dm, o)
+    prog = rec.program
+
+    def step():
+        dm.reset()
+        prog.run(dm)
+        return dm.trace()            # waits for the stream
+
+    step()
+    ts = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        step()
+        ts.append(time.perf_counter() - t0)
+    ms = 1e3 * min(ts)
+    d = dm.get_diagonal()
+    bits = (np.arange(1 << n)[:, None] >> np.arange(n)[None, :]) & 1
+    zz = [float((d * (1 - 2 * bits[:, i]) * (1 - 2 * bits[:, i + 1])).sum()) for i in range(n - 1)]
+    op_bytes = 2.0 * 16.0 * float(4 ** n)
+    out = {"workload": f"density matrix {n}q noisy brick-wall depth {depth} ({len(ops)} unitary / Kraus operations), "
+                       "complex128", "ops": len(ops), "passes": prog.passes, "circuit_ms": round(ms, 2),
+           "ops_per_s": round(len(ops) / (ms / 1e3), 1),
+           "GBs_per_pass": round(prog.passes * op_bytes / (ms / 1e3) / 1e9, 1),
+           "trace": dm.trace(), "purity": dm.purity(), "zz_mean": float(np.mean(zz)), "zz_first": zz[:3]}
+    del prog
+    dm.close()
+    try:
+        core = RefCore()
+    except FileNotFoundError:
+        out["cpu"] = "reference core not built"
+        return out
+    avail = 0
+    for line in open("/proc/meminfo"):
+        if line.startswith("MemAvailable"):
+            avail = int(line.split()[1]) * 1024
+    if avail < 3 * 16 * 4 ** n:
+        out["cpu"] = "not enough host memory for the 4 GiB reference density matrix and its temporaries"
+        return out
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    ref = core.dm(n)
+    done, t0 = 0, time.perf_counter()
+    for o in ops:
+        apply(ref, o)
+        done += 1
+        if time.perf_counter() - t0 > args.dm_cpu_seconds:
+            break
+    cpu_s = time.perf_counter() - t0
+    rate = done / cpu_s
+    out.update({"cpu_ops_per_s": round(rate, 3), "cpu_kind": "reference", "cpu_cores": threads,
+                "cpu_sample": f"first {done} operations of the circuit, {cpu_s:.1f} s",
+                "cpu_circuit_s_estimate": round(len(ops) / rate, 1),
+                "speedup_vs_cpu": round((len(ops) / rate) / (ms / 1e3), 1)})
+    return out
+
+
+def adjoint30_section(args):
+    """One 30-qubit adjoint gradient: 16 layers of RY and RZ on every qubit
+    plus a CZ ring (960 parameters), TFIM H with h = 0.7, complex128; the
+    gradient is checked against the parameter-shift rule on 4 parameters."""
+    from invariantq_b200.gradients import Ansatz, PauliHamiltonian, adjoint_gradient, adjoint_stats, ansatz_energies
+    from invariantq_b200.gradients import shifted_parameter_sets
+    n, L = 30, 16
+    a, h = Ansatz.hardware_efficient(n, L), PauliHamiltonian.tfim(n, 0.7)
+    rng = np.random.default_rng(30)
+    th = rng.uniform(0, 2 * np.pi, a.num_params)
+    adjoint_gradient(a, h, th)                     # warm-up: planning, workspace
+    t0 = time.perf_counter()
+    e, g = adjoint_gradient(a, h, th)
+    t = time.perf_counter() - t0
+    st = adjoint_stats()
+    idx = rng.choice(a.num_params, 4, replace=False)
+    sets = shifted_parameter_sets(th)
+    rows = np.concatenate([[2 * j, 2 * j + 1] for j in idx])
+    es = ansatz_energies(a, h, sets[rows])
+    ps = 0.5 * (es[0::2] - es[1::2])
+    return {"workload": f"{n}q, {L} layers RY+RZ per qubit + CZ ring ({a.num_params} parameters), TFIM h=0.7, complex128; "
+                        "three state-sized buffers (psi and the 2^(n+1) psi/lambda array), no checkpoints",
+            "gradient_s": round(t, 3), "energy": e, "passes": {"forward": int(st["forward_passes"]),
+                                                              "backward": int(st["backward_passes"])},
+            "achieved_gbs": round(st["bytes"] / t / 1e9, 1),
+            "max_abs_diff_vs_param_shift": float(np.max(np.abs(ps - g[idx]))), "checked_parameters": [int(i) for i in idx]}
+
+
 # ---------------------------------------------------------------- our arm
 
 def our_arm(args, rank, world, local_rank):
@@ -328,7 +553,7 @@ def our_arm(args, rank, world, local_rank):
     gates = circuit_gates(n, args.depth, args.seed)
     sv = NativeStateVector(n)
     for key, val in (("tile_bits", args.tile_bits), ("chunk_bits", args.chunk_bits), ("budget", args.budget),
-                     ("max_stages", args.max_stages), ("nbuf", args.nbuf)):
+                     ("max_stages", args.max_stages), ("nbuf", args.nbuf), ("reg_slots", args.reg_slots)):
         if val is not None:
             sv.set_option(key, val)
     with sv.record() as rec:
@@ -403,6 +628,14 @@ def our_arm(args, rank, world, local_rank):
         assert np.all(np.abs(z) <= 1.0 + 1e-9)
 
     adj = adjoint_section(args, rank, world) if not args.no_adjoint else None
+    opts = {k: sv.get_option(k) for k in ("tile_bits", "chunk_bits", "budget", "max_stages", "nbuf", "reg_slots")}
+    configs = None
+    if world == 1 and not args.no_configs:
+        configs = {"fusion_sweep_30q": fusion_sweep_section(args, sv, n, stream),
+                   "brickwall_20q": brickwall20_section(args)}
+        sv.close()
+        configs["density_matrix_14q"] = density_matrix_section(args)
+        configs["adjoint_30q"] = adjoint30_section(args)
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
@@ -419,9 +652,7 @@ def our_arm(args, rank, world, local_rank):
                                f"complex128, planned into tile passes",
                    "qubits": n, "depth": args.depth, "gates": len(gates), "passes": prog.passes,
                    "gates_per_pass": round(len(gates) / prog.passes, 2),
-                   "tile_bits": sv.get_option("tile_bits"), "chunk_bits": sv.get_option("chunk_bits"),
-                   "budget": sv.get_option("budget"), "max_stages": sv.get_option("max_stages"),
-                   "nbuf": sv.get_option("nbuf"),
+                   **opts,
                    "l2": "state (16 B x 2^n) larger than the 126 MB L2; no flush between steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "circuit_ms": round(ms / args.steps, 3),
@@ -437,6 +668,8 @@ def our_arm(args, rank, world, local_rank):
     }
     if adj is not None:
         out["adjoint"] = adj
+    if configs is not None:
+        out["configs"] = configs
     if world == 1 and not args.no_cpu_baseline:
         gbs, done, nq, kind, threads, dt = cpu_reference_run(gates, n, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": kind,

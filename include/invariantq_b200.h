@@ -135,8 +135,10 @@ void* iq_statevector_stream(void* sv);
 size_t iq_statevector_num_qubits(void* sv);
 
 /* Tuning / diagnostics for either handle kind.  Keys: "tile_bits", "chunk_bits",
- * "reg_slots", "max_stages", "budget", "nbuf", "ctas_per_sm", "eager",
- * "flush_ops", "profile".  0 = ok, -1 = unknown key or bad value. */
+ * "reg_slots" (register slots R = 3, 4, 5 per tile-pass thread: 2^R amplitudes
+ * each; raised to the widest fused block), "max_stages", "budget", "nbuf",
+ * "ctas_per_sm", "eager", "fuse", "flush_ops", "profile".  0 = ok, -1 =
+ * unknown key or bad value. */
 int iq_handle_set_option(void* h, const char* key, double value);
 double iq_handle_get_option(void* h, const char* key);
 /* Counters: out[0] passes, [1] operations applied, [2] algorithmic bytes moved by

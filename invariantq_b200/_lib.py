@@ -11,7 +11,7 @@ import os
 from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = Path(os.environ.get("IQ_LIBRARY", _PKG / "libinvariantq.so"))
+LIB_PATH = Path(os.environ.get("IQ_LIBRARY") or _PKG / "libinvariantq.so")
 
 c_dp = ctypes.POINTER(ctypes.c_double)
 c_u64p = ctypes.POINTER(ctypes.c_uint64)

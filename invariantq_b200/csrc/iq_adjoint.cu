@@ -66,7 +66,7 @@ struct Cfg {
     Cfg c;
     c.sp.M = env_int("IQ_TILE_BITS", 11);
     c.sp.c = env_int("IQ_CHUNK_BITS", 5);
-    c.sp.R = 4;
+    c.sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
     c.sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
     c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
@@ -188,7 +188,7 @@ bool make_shape(const Cfg& cfg, int nbits, const std::vector<SchedOp>& fused, si
   p.nbits = nbits;
   int maxk = 1;
   for (const SchedOp& o : fused) maxk = std::max<int>(maxk, o.k);
-  p.R = maxk > 4 ? 5 : 4;
+  p.R = std::min(5, std::max(cfg.sp.R, maxk));
   if (plan_passes(p, fused, s.plans, err) < 0) return false;
   std::vector<cplx64> idx(pool_size), packed;
   for (size_t i = 0; i < pool_size; ++i) idx[i] = {(double)i, 0.0};

@@ -29,8 +29,8 @@ __device__ __forceinline__ double2 ld_mat(const double2* m, int i) { return m[i]
 constexpr int kMaxBuf = 4;
 
 // tile buffers + alignment slack + this pass's matrix block
-size_t tile_pass_smem_bytes(int M, int nbuf, uint32_t mat_elems, uint32_t ngrad) {
-  return (size_t)nbuf * (16u << M) + 1024 + (size_t)mat_elems * 16 + (size_t)ngrad * (kTileThreads / 8) * 8;
+size_t tile_pass_smem_bytes(int M, int R, int nbuf, uint32_t mat_elems, uint32_t ngrad) {
+  return (size_t)nbuf * (16u << M) + 1024 + (size_t)mat_elems * 16 + (size_t)ngrad * (tile_pass_threads(R) / 8) * 8;
 }
 
 
@@ -43,9 +43,10 @@ unsigned tile_pass_grid(const PassDesc& d, const TileLaunch& tl, int num_sms) {
 cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
                              const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials) {
   const int nbuf = tl.nbuf < 1 ? 1 : (tl.nbuf > kMaxBuf ? kMaxBuf : tl.nbuf);
-  const size_t smem = tile_pass_smem_bytes(d.M, nbuf, d.mat_elems, d.ngrad);
+  const size_t smem = tile_pass_smem_bytes(d.M, d.R, nbuf, d.mat_elems, d.ngrad);
   const unsigned grid = tile_pass_grid(d, tl, num_sms);
   if (d.ngrad && !grad_partials) return cudaErrorInvalidValue;
+  if (d.R == 3) return launch_tile_r3(tm, d, mats, dev_status, nbuf, grid, smem, st, grad_partials);
   if (d.R == 4) return launch_tile_r4(tm, d, mats, dev_status, nbuf, grid, smem, st, grad_partials);
   return launch_tile_r5(tm, d, mats, dev_status, nbuf, grid, smem, st, grad_partials);
 }

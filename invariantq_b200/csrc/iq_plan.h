@@ -107,7 +107,7 @@ struct SchedParams {
   int nbits;             // index bits of the array (SV: n, DM: 2n)
   int M;                 // tile bits
   int c;                 // contiguous chunk bits (>= 3)
-  int R;                 // register slots per thread (4 or 5)
+  int R;                 // register slots per thread (3, 4 or 5)
   int max_stages;        // stages per pass (each costs one shared-memory round trip)
   double budget;         // max arithmetic cost per pass (real FMAs per amplitude)
   double grad_cost = 6.0;    // cost of an adjoint step: a structured rotation on both halves (4) plus its products

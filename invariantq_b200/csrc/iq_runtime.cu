@@ -240,7 +240,7 @@ struct Engine {
     tl.consumers = 128;
     sp.M = env_int("IQ_TILE_BITS", 11);
     sp.c = env_int("IQ_CHUNK_BITS", 5);
-    sp.R = 4;
+    sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));   // register slots (R); wider blocks raise it
     sp.max_stages = env_int("IQ_MAX_STAGES", 8);
     sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
@@ -397,7 +397,7 @@ struct Engine {
     } else {
       SchedParams p = sp;
       p.nbits = nbits;
-      p.R = maxk > 4 ? 5 : 4;
+      p.R = std::min(5, std::max(sp.R, maxk));
       std::string err;
       if (plan_passes(p, fused, pg.plans, err) < 0) {
         set_error(E_STATE, "scheduler: %s", err.c_str());
@@ -1059,6 +1059,7 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "max_stages")) { if (iv < 1 || iv > kMaxStages) return -1; e->sp.max_stages = iv; }
   else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; }
   else if (!strcmp(key, "nbuf")) { if (iv < 1 || iv > 4) return -1; e->tl.nbuf = iv; }
+  else if (!strcmp(key, "reg_slots")) { if (iv < 3 || iv > 5) return -1; e->sp.R = iv; }
   else if (!strcmp(key, "ctas_per_sm")) { if (iv < 1 || iv > 4) return -1; e->tl.ctas_per_sm = iv; }
   else if (!strcmp(key, "consumers")) { if (iv != 128) return -1; e->tl.consumers = iv; }
   else if (!strcmp(key, "eager")) e->eager = iv ? 1 : 0;
@@ -1077,6 +1078,7 @@ double iq_handle_get_option(void* h, const char* key) {
   if (!strcmp(key, "max_stages")) return e->sp.max_stages;
   if (!strcmp(key, "budget")) return e->sp.budget;
   if (!strcmp(key, "nbuf")) return e->tl.nbuf;
+  if (!strcmp(key, "reg_slots")) return e->sp.R;
   if (!strcmp(key, "ctas_per_sm")) return e->tl.ctas_per_sm;
   if (!strcmp(key, "consumers")) return e->tl.consumers;
   if (!strcmp(key, "eager")) return e->eager;

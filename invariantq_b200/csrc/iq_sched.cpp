@@ -213,7 +213,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
                 std::string& err) {
   const int nb = p.nbits;
   const int nops = (int)ops.size();
-  if (p.R < 4 || p.R > kMaxK) { err = "register slots must be 4 or 5"; return -1; }
+  if (p.R < 3 || p.R > kMaxK) { err = "register slots must be 3, 4 or 5"; return -1; }
   if (nb < p.R + kLaneBits) { err = "array too small for the tile kernel"; return -1; }
   const int M = std::min(p.M, nb);
   const bool whole = nb <= p.M;         // the whole array is one tile

@@ -569,7 +569,7 @@ __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int 
 #pragma unroll
     for (int v = 0; v < NV; ++v) a[v] = tile[base ^ voff<R>(v, sb)];
     bool stored = false;
-    if constexpr (R == 4) {
+    if constexpr (R <= 4) {
       // ops alternate a -> b, b -> a; an odd count ends with a plain copy back
       // (two inlined dispatch sites only)
       double2 b[NV];

@@ -7,11 +7,11 @@ namespace iqb {
 
 cudaError_t launch_tile_r5(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status, int nbuf,
                           unsigned grid, size_t smem, cudaStream_t st, double* grad_partials) {
-  auto kern = tile_pass_kernel<5, kTileThreads, 1>;
+  auto kern = tile_pass_kernel<5, tile_pass_threads(5), 1>;
   static std::atomic<uint64_t> smem_set{0};
   cudaError_t r = allow_full_dynamic_smem(kern, smem_set);
   if (r != cudaSuccess) return r;
-  kern<<<grid, kTileThreads, smem, st>>>(tm, d, mats, dev_status, nbuf, grad_partials);
+  kern<<<grid, tile_pass_threads(5), smem, st>>>(tm, d, mats, dev_status, nbuf, grad_partials);
   return cudaGetLastError();
 }
 

@@ -270,8 +270,8 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
 // (n characters per term, character q acting on qubit q).
 extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
                            const double* params, int nterms, const double* coeffs, const char* paulis, int M, int c,
-                           int max_stages, double budget, double* energy, double* grad, int nparams, char* errbuf,
-                           int errlen) {
+                           int R, int max_stages, double budget, double* energy, double* grad, int nparams,
+                           char* errbuf, int errlen) {
   std::vector<AnsatzOp> ops(nops);
   for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
   std::string err;
@@ -290,7 +290,7 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
   ansatz_forward(n, ops, params, fw, pool);
   f.pool.assign(reinterpret_cast<const cd*>(pool.data()), reinterpret_cast<const cd*>(pool.data()) + pool.size());
   if (n >= 7) {
-    if (run_plan(f, fw, M, c, 4, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+    if (run_plan(f, fw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
   } else {   // the runtime's one-operation kernel: dense matrix, LSB-first qubit list
     for (const SchedOp& o : fw) {
       const int d = 1 << o.k;
@@ -348,7 +348,7 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
   ansatz_backward(n, ops, params, bw, bpool, gp);
   b.pool.assign(reinterpret_cast<const cd*>(bpool.data()), reinterpret_cast<const cd*>(bpool.data()) + bpool.size());
   b.grads.assign(gp.size(), 0.0);
-  if (run_plan(b, bw, M, c, 4, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+  if (run_plan(b, bw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
   for (int p = 0; p < nparams; ++p) grad[p] = 0.0;
   for (size_t t = 0; t < gp.size(); ++t) grad[gp[t]] += b.grads[t];
   return 0;

@@ -25,7 +25,7 @@ def emu(tmp_path_factory):
     return ctypes.CDLL(str(out))
 
 
-def emu_grad(emu, n, ops, theta, coeffs, paulis, M=11, c=5, stages=8, budget=80.0):
+def emu_grad(emu, n, ops, theta, coeffs, paulis, M=11, c=5, stages=8, budget=80.0, R=4):
     k = np.array([o[0] for o in ops], np.int32)
     q0 = np.array([o[1] for o in ops], np.int32)
     q1 = np.array([o[2] for o in ops], np.int32)
@@ -38,7 +38,7 @@ def emu_grad(emu, n, ops, theta, coeffs, paulis, M=11, c=5, stages=8, budget=80.
     err = ctypes.create_string_buffer(256)
     P = ctypes.c_void_p
     rc = emu.emu_adjoint(n, len(ops), P(k.ctypes.data), P(q0.ctypes.data), P(q1.ctypes.data), P(pi.ctypes.data),
-                         P(th.ctypes.data), len(coeffs), P(co.ctypes.data), ps, M, c, stages, ctypes.c_double(budget),
+                         P(th.ctypes.data), len(coeffs), P(co.ctypes.data), ps, M, c, R, stages, ctypes.c_double(budget),
                          ctypes.byref(e), P(g.ctypes.data), len(theta), err, 256)
     assert rc == 0, err.value
     return e.value, g
@@ -65,5 +65,18 @@ def test_mixed_gates_gradient(port, emu, n, ngates, seed):
     paulis = ["".join(rng.choice(list("IXYZ"), n)) for _ in range(6)]
     coeffs = rng.normal(size=6)
     e, g = emu_grad(emu, n, ops, theta, coeffs, paulis, budget=60.0, stages=4)
+    assert abs(e - ar.energy(port, n, ops, theta, coeffs, paulis)) < 1e-12
+    assert np.max(np.abs(g - ar.param_shift(port, n, ops, theta, coeffs, paulis))) < 1e-10
+
+
+@pytest.mark.parametrize("R", [3, 5])
+def test_register_slot_variants(port, emu, R):
+    """Adjoint steps keep the select bit in slot 0 with 3 and 5 register slots."""
+    n, layers = 8, 2
+    rng = np.random.default_rng(20 + R)
+    ops = ar.tfim_ops(n, layers)
+    theta = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
+    coeffs, paulis = tfim_terms(n, 0.7)
+    e, g = emu_grad(emu, n, ops, theta, coeffs, paulis, R=R)
     assert abs(e - ar.energy(port, n, ops, theta, coeffs, paulis)) < 1e-12
     assert np.max(np.abs(g - ar.param_shift(port, n, ops, theta, coeffs, paulis))) < 1e-10

@@ -127,6 +127,22 @@ def test_tile_configurations(SV, port, M, c, budget, stages, nbuf):
     assert np.max(np.abs(sv.get_amplitudes() - ref)) < TOL
 
 
+@pytest.mark.parametrize("n,M,c,budget,stages,nbuf", [(9, 11, 5, 80, 8, 3), (16, 11, 5, 80, 8, 3),
+                                                      (18, 10, 5, 40, 6, 2), (18, 12, 6, 120, 8, 2)])
+def test_three_register_slots(SV, port, n, M, c, budget, stages, nbuf):
+    """The 256-thread R = 3 tile kernel (operations of width <= 3) against the oracle."""
+    rng = np.random.default_rng(n * 7 + M)
+    ops = gen_ops(rng, n, 150, kmax=3)
+    ref = oracle_apply(port, port.zero_state(n), n, ops)
+    sv = SV(n)
+    for k, v in (("reg_slots", 3), ("tile_bits", M), ("chunk_bits", c), ("budget", budget), ("max_stages", stages),
+                 ("nbuf", nbuf)):
+        sv.set_option(k, v)
+    assert sv.get_option("reg_slots") == 3
+    apply_abi(sv, ops)
+    assert np.max(np.abs(sv.get_amplitudes() - ref)) < TOL
+
+
 def test_five_qubit_blocks(SV):
     """k = 5 fused blocks (the reference stops at 4) against a numpy contraction."""
     from tests.test_scheduler_emulated import apply_lsb_numpy

@@ -125,6 +125,9 @@ def oracle_apply(port, state, n, ops):
     (15, 12, 7, 4, 3, 30.0, 6),
     (16, 13, 5, 4, 8, 200.0, 7),
     (14, 12, 5, 5, 8, 500.0, 8),    # five register slots
+    (10, 10, 5, 3, 8, 80.0, 9),     # three register slots (256-thread variant)
+    (13, 11, 5, 3, 6, 60.0, 10),
+    (14, 11, 6, 3, 8, 120.0, 11),
 ])
 def test_emulated_passes_match_oracle(port, emu, n, M, c, R, stages, budget, seed):
     rng = np.random.default_rng(seed)
@@ -168,3 +171,16 @@ def test_brickwall_pass_count_and_parity(port, emu):
     assert np.max(np.abs(got - ref)) < 1e-12
     # far fewer passes than gates
     assert npasses < len(ops) / 4
+
+
+@pytest.mark.parametrize("R", [3, 4])
+def test_brickwall_register_slots(port, emu, R):
+    """The brick-wall planned with 3 and 4 register slots gives the oracle's state."""
+    n, depth = 15, 6
+    ops = brickwall_ops(n, depth, 1)
+    ref = np.zeros(1 << n, np.complex128)
+    ref[0] = 1
+    start = ref.copy()
+    ref = oracle_apply(port, ref, n, ops)
+    got, npasses, per = run_emu(emu, n, [to_lsb(*o) for o in ops], start, M=11, c=5, R=R)
+    assert np.max(np.abs(got - ref)) < 1e-12
