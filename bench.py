@@ -453,6 +453,15 @@ def density_matrix_section(args):
         else:
             target.apply_1q_kraus(qs[0], m)
 
+    def apply_ref(target, o):       # the reference core's wrapper names
+        kind, qs, m = o
+        if kind == "u1":
+            target.apply_1q(qs[0], m)
+        elif kind == "u2":
+            target.apply_2q(qs[0], qs[1], m)
+        else:
+            target.apply_kraus_1q(qs[0], m)
+
     dm = NativeDensityMatrix(n)
     with dm.record() as rec:
         for o in ops:
@@ -498,7 +507,7 @@ def density_matrix_section(args):
     ref = core.dm(n)
     done, t0 = 0, time.perf_counter()
     for o in ops:
-        apply(ref, o)
+        apply_ref(ref, o)
         done += 1
         if time.perf_counter() - t0 > args.dm_cpu_seconds:
             break
