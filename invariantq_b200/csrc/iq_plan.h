@@ -205,6 +205,56 @@ IQ_HD void chunk_coords(uint64_t A, const PassDesc& P, int& c1, int& c2, int& c3
   }
 }
 
+// Tensor-map coordinates of tile t's first copy, computed from t directly
+// (equal to chunk_coords(tile_base(t, P), P)).  The tile index's bits fill the
+// non-tile bit positions in order; cut at H[0] and H[1] they give: the low
+// n1 = H0 - c bits -> dim 1 (above the chunk's 2^(c-3) rows), the next
+// n3 = H1 - H0 - 1 bits -> dim 3, the rest -> the top dimension with the
+// higher tile bits as zero gaps.  Built once per thread; 32-bit arithmetic.
+struct TileCoordMap {
+  int nbox;
+  int n1, sh1;            // dim 1: (t & ((1 << n1) - 1)) << sh1
+  int n3;                 // dim 3 (nbox 2): (t >> n1) & ((1 << n3) - 1)
+  int shhi;               // top-dimension bits start at t >> shhi
+  int ngap;
+  uint8_t gap[kMaxTileBits];   // ascending zero positions in the top coordinate
+};
+
+IQ_HD void tile_coord_map(const PassDesc& P, TileCoordMap& m) {
+  m.nbox = P.nbox;
+  m.ngap = 0;
+  if (P.nbox == 0) {       // the chunk alone: dim 1 = A >> 3 = t << (c - 3)
+    m.n1 = 31; m.sh1 = P.c - 3; m.n3 = 0; m.shhi = 31;
+    return;
+  }
+  const int h0 = P.H[0];
+  m.n1 = h0 - P.c;
+  m.sh1 = P.c - 3;
+  const int lo = (P.nbox == 2) ? P.H[1] : h0;   // the top dimension starts at this bit
+  m.n3 = (P.nbox == 2) ? P.H[1] - h0 - 1 : 0;
+  m.shhi = m.n1 + m.n3;
+  m.gap[m.ngap++] = 0;                          // bit `lo` itself is a tile bit
+  for (int i = P.nbox; i < P.nH; ++i) m.gap[m.ngap++] = (uint8_t)(P.H[i] - lo);
+}
+
+IQ_HD void tile_coords(uint32_t t, const TileCoordMap& m, int& c1, int& c2, int& c3, int& c4) {
+  c1 = (int)((m.n1 >= 31 ? t : (t & ((1u << m.n1) - 1u))) << m.sh1);
+  c2 = c3 = c4 = 0;
+  if (m.nbox == 0) return;
+  uint32_t x = m.shhi >= 32 ? 0u : (t >> m.shhi);
+  for (int i = 0; i < kMaxTileBits; ++i)
+    if (i < m.ngap) {
+      const int g = m.gap[i];
+      x = ((x >> g) << (g + 1)) | (x & ((1u << g) - 1u));
+    }
+  if (m.nbox == 2) {
+    c3 = (int)((t >> m.n1) & ((1u << m.n3) - 1u));
+    c4 = (int)x;
+  } else {
+    c2 = (int)x;
+  }
+}
+
 }  // namespace iqb
 
 #ifdef __cplusplus

@@ -87,6 +87,23 @@ __device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity
       : "memory");
   return done;
 }
+
+// try_wait that lets the hardware park the thread until the phase completes or
+// `hint_ns` passes, so a waiting warp issues no instructions meanwhile (a plain
+// try_wait returns almost at once and the polling loop would take issue slots
+// from the warps that compute)
+constexpr uint32_t kWaitSuspendNs = 20000;
+__device__ __forceinline__ uint32_t mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return done;
+}
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -129,7 +146,7 @@ __device__ __forceinline__ uint64_t global_ns() {
 // flight land before the CTA exits after an abort.
 __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity) {
   const uint64_t t0 = global_ns();
-  while (!mbar_try_wait(bar, parity))
+  while (!mbar_try_wait_suspend(bar, parity, kWaitSuspendNs))
     if (global_ns() - t0 > kWaitLimitNs) return;
 }
 
@@ -141,7 +158,7 @@ __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, vol
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (;;) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_suspend(bar, parity, kWaitSuspendNs)) return true;
     if (*abort_flag) return false;
     if (global_ns() - t0 > kWaitLimitNs) break;
   }
@@ -534,10 +551,39 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
     }
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
-    case OP_D2R: disp_d2r<R, IP>(od.a, od.b, s, d, m); break;
+    case OP_D2R:
+      // one jump over the ordered slot pair (a, b) instead of nested compares
+      switch (od.a * 8 + od.b) {
+#define IQ_D2R_CASE(A, B)                                               \
+  case A * 8 + B:                                                       \
+    if constexpr (A < R && B < R && A != B) d2r<R, A, B, IP>(s, d, m); \
+    break;
+        IQ_D2R_CASE(0, 1) IQ_D2R_CASE(0, 2) IQ_D2R_CASE(0, 3) IQ_D2R_CASE(0, 4)
+        IQ_D2R_CASE(1, 0) IQ_D2R_CASE(1, 2) IQ_D2R_CASE(1, 3) IQ_D2R_CASE(1, 4)
+        IQ_D2R_CASE(2, 0) IQ_D2R_CASE(2, 1) IQ_D2R_CASE(2, 3) IQ_D2R_CASE(2, 4)
+        IQ_D2R_CASE(3, 0) IQ_D2R_CASE(3, 1) IQ_D2R_CASE(3, 2) IQ_D2R_CASE(3, 4)
+        IQ_D2R_CASE(4, 0) IQ_D2R_CASE(4, 1) IQ_D2R_CASE(4, 2) IQ_D2R_CASE(4, 3)
+#undef IQ_D2R_CASE
+        default: break;
+      }
+      break;
     case OP_M1R: disp_m1r<R>(od.a, s, d, m, od.perm, unit); break;
     case OP_M1L: m1l<R>(s, d, m, od.a, lane8, omask, od.perm, unit); break;
-    case OP_M2R: disp_m2r<R>(od.a, od.b, s, d, m, od.perm, unit); break;
+    case OP_M2R:
+      switch (od.a * 8 + od.b) {
+#define IQ_M2R_CASE(A, B)                                                          \
+  case A * 8 + B:                                                                  \
+    if constexpr (A < R && B < R && A != B) m2r<R, A, B>(s, d, m, od.perm, unit); \
+    break;
+        IQ_M2R_CASE(0, 1) IQ_M2R_CASE(0, 2) IQ_M2R_CASE(0, 3) IQ_M2R_CASE(0, 4)
+        IQ_M2R_CASE(1, 0) IQ_M2R_CASE(1, 2) IQ_M2R_CASE(1, 3) IQ_M2R_CASE(1, 4)
+        IQ_M2R_CASE(2, 0) IQ_M2R_CASE(2, 1) IQ_M2R_CASE(2, 3) IQ_M2R_CASE(2, 4)
+        IQ_M2R_CASE(3, 0) IQ_M2R_CASE(3, 1) IQ_M2R_CASE(3, 2) IQ_M2R_CASE(3, 4)
+        IQ_M2R_CASE(4, 0) IQ_M2R_CASE(4, 1) IQ_M2R_CASE(4, 2) IQ_M2R_CASE(4, 3)
+#undef IQ_M2R_CASE
+        default: break;
+      }
+      break;
     case OP_DKR: disp_dkr<R>(od.k, s, m, tile, sb, base); return true;
     default: break;
   }
@@ -570,18 +616,25 @@ __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int 
     for (int v = 0; v < NV; ++v) a[v] = tile[base ^ voff<R>(v, sb)];
     bool stored = false;
     if constexpr (R <= 4) {
-      // ops alternate a -> b, b -> a; an odd count ends with a plain copy back
-      // (two inlined dispatch sites only)
+      // ops alternate a -> b, b -> a (two inlined dispatch sites only); after an
+      // odd count the result is in b and is stored from there
       double2 b[NV];
+      bool inb = false;
       for (int o = op0; o < op1; o += 2) {
         stored |= apply_op<R, false>(P.ops[o], a, b, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
-        if (o + 1 < op1) {
-          stored |= apply_op<R, false>(P.ops[o + 1], b, a, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
-        } else if (!stored) {
+        if (o + 1 < op1) stored |= apply_op<R, false>(P.ops[o + 1], b, a, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
+        else inb = true;
+      }
+      if (!stored) {
+        if (inb) {
 #pragma unroll
-          for (int v = 0; v < NV; ++v) a[v] = b[v];
+          for (int v = 0; v < NV; ++v) tile[base ^ voff<R>(v, sb)] = b[v];
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) tile[base ^ voff<R>(v, sb)] = a[v];
         }
       }
+      continue;
     } else {
       for (int o = op0; o < op1; ++o) stored |= apply_op<R, true>(P.ops[o], a, a, mats, lane8, omask, tile, sb, base, sgrad, P.grad_base);
     }
@@ -659,20 +712,11 @@ __global__ void __launch_bounds__(NT, MINB)
     else jc1[r] = jc3[r] = jc4[r] = 0;
   }
   for (int j = warp; j < nissue; j += NW) my_bytes += box_bytes;
-  int Hr[kMaxTileBits];
-#pragma unroll
-  for (int i = 0; i < kMaxTileBits; ++i) Hr[i] = P.H[i];
-  const int nH = P.nH, cb = P.c;
+  TileCoordMap cmap;               // tile index -> tensor-map coordinates (32-bit, per thread)
+  tile_coord_map(P, cmap);
   auto base_coords = [&](uint64_t t, int& c1, int& c3, int& c4) {
-    uint64_t x = t << cb;
-#pragma unroll
-    for (int i = 0; i < kMaxTileBits; ++i)
-      if (i < nH) {
-        const int h = Hr[i];
-        x = ((x >> h) << (h + 1)) | (x & ((1ULL << h) - 1));
-      }
     int c2;
-    chunk_coords(x, P, c1, c2, c3, c4);
+    tile_coords((uint32_t)t, cmap, c1, c2, c3, c4);
   };
   auto issue_load = [&](uint64_t i) {   // whole warp, converged
     const int b = (int)(i % nbuf);
