@@ -224,10 +224,16 @@ int iq_adjoint_gradient(size_t num_qubits, size_t num_ops, const int* kinds, con
                         const int* param_index, size_t num_params, const double* params, size_t num_terms,
                         const double* coeffs, const char* paulis, double* energy_out, double* grad_out);
 /* Every parameter set of every circuit, run concurrently on num_streams CUDA
- * streams (<= 0: IQ_ADJOINT_STREAMS or 8), each with its own device workspace
- * sized for the largest circuit; fewer streams when the workspaces would not
- * fit in device memory.  Returns 0, or -1 with iq_last_error set. */
+ * streams (<= 0: IQ_ADJOINT_STREAMS or 8), each with its own device workspace;
+ * the parameter sets of one circuit run together, through the same tile-pass
+ * launches, in groups that fit IQ_ADJOINT_JOB_BYTES (4 GiB) of states.  Fewer
+ * streams when the workspaces would not fit in device memory.  Workspaces are
+ * kept for later calls unless they hold more than 8 GiB of device memory.
+ * Returns 0, or -1 with iq_last_error set. */
 int iq_adjoint_gradient_batch(const iq_adjoint_circuit* circuits, size_t num_circuits, int num_streams);
+/* Free the device and pinned host memory the adjoint calls keep between calls;
+ * returns the number of workspaces freed. */
+int iq_adjoint_release(void);
 /* Energies only (grad_out unused): the forward circuit and <psi|H|psi> for each
  * parameter set of one circuit, one set after another on one stream -- the
  * plain path a parameter-shift gradient evaluates 2 x num_params times. */

@@ -113,6 +113,7 @@ SIGNATURES = {
     "iq_adjoint_gradient_batch": ([ctypes.POINTER(AdjointCircuit), _sz, _i], _i),
     "iq_ansatz_energy": ([ctypes.POINTER(AdjointCircuit)], _i),
     "iq_adjoint_stats": ([c_dp, _sz], _i),
+    "iq_adjoint_release": ([], _i),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),
     "iq_density_matrix_get_diagonal": ([_v, c_dp], None),

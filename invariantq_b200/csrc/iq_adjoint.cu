@@ -36,6 +36,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -262,10 +263,12 @@ struct DevBuf {
   T* p = nullptr;
   size_t cap = 0;
   // grow to n elements; `user` (the stream that reads the buffer) is drained before the old one is freed
+  // (growth doubles: allocation calls synchronise the whole device)
   bool ensure(size_t n, std::string& err, const char* what, cudaStream_t user = nullptr) {
     if (n <= cap) return true;
     if (p && user) cudaStreamSynchronize(user);
     if (p) cudaFree(p);
+    n = std::max(n, 2 * cap);
     p = nullptr;
     cap = 0;
     if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
@@ -286,6 +289,7 @@ struct HostBuf {
   bool ensure(size_t n, std::string& err) {
     if (n <= cap) return true;
     if (p) cudaFreeHost(p);
+    n = std::max(n, 2 * cap);
     p = nullptr;
     cap = 0;
     if (cudaMallocHost(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) {
@@ -303,7 +307,7 @@ struct HostBuf {
 struct Pending {
   bool active = false;
   Circuit* c = nullptr;
-  size_t set = 0;
+  std::vector<size_t> sets;   // parameter sets in launch order (device set k = sets[k])
   std::vector<int> grad_param;
   int ngrads = 0;
   bool grad = false;
@@ -317,29 +321,56 @@ struct Workspace {
   DevBuf<uint64_t> zmask;
   DevBuf<int> status;
   HostBuf<double2> hmats[2];
-  HostBuf<double> hout[2];    // energy, then the gradient terms
+  HostBuf<double> hout[2];    // energies of the job's sets, then their gradient terms
   HostBuf<int> hstat[2];      // device status word
   cudaEvent_t ev[2] = {nullptr, nullptr};
   Pending pend[2];
   int slot = 0;
-  std::unordered_map<const Shape*, std::vector<CUtensorMap>> tmaps;
+  std::map<std::pair<const Shape*, uint32_t>, std::vector<CUtensorMap>> tmaps;   // (shape, sets)
   const Circuit* ham_of = nullptr;   // circuit whose Hamiltonian tables are on the device
 
-  bool init(int dev, int sms, int nmax, std::string& err) {
-    device = dev;
-    num_sms = sms;
-    if (cudaSetDevice(dev) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+  // The state arrays are sized up front for the batch's largest job; matrix,
+  // partial and staging buffers grow on demand (doubling, so a worker
+  // reallocates a few times at the start: the largest jobs run first).
+  struct Bounds {
+    uint64_t psi_amps = 1, joint_amps = 1;
+    size_t mats = 1, sets = 1, grads = 1;   // per job: matrix elements, sets, gradient terms x sets
+  };
+
+  // Make ready for a call on device `dev` (a workspace can come back from the
+  // pool of an earlier call: pointers into that call's shapes and circuits are
+  // dropped, buffers are kept when large enough).
+  bool prepare(int dev, int sms, const Bounds& bd, std::string& err) {
+    if (!stream) {
+      device = dev;
+      num_sms = sms;
+      if (cudaSetDevice(dev) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        err = "cannot create a CUDA stream or event";
+        return false;
+      }
+    } else if (cudaSetDevice(dev) != cudaSuccess) {
       cudaGetLastError();
-      err = "cannot create a CUDA stream or event";
+      err = "cudaSetDevice failed";
       return false;
     }
-    if (!psi.ensure(1ULL << nmax, err, "the state") || !joint.ensure(1ULL << joint_bits(nmax), err, "the joint array") ||
-        !red.ensure(kRedBlocks + 8, err, "reduction partials") || !status.ensure(1, err, "the status word"))
+    tmaps.clear();
+    ham_of = nullptr;
+    slot = 0;
+    pend[0].active = pend[1].active = false;
+    if (!psi.ensure(bd.psi_amps, err, "the states", stream) ||
+        !joint.ensure(bd.joint_amps, err, "the joint arrays", stream) || !status.ensure(1, err, "the status word") ||
+        !red.ensure(bd.sets * (kRedBlocks + 1), err, "reduction partials", stream))
       return false;
     return cudaMemsetAsync(status.p, 0, sizeof(int), stream) == cudaSuccess;
+  }
+
+  double device_bytes() const {
+    return 16.0 * ((double)psi.cap + (double)joint.cap + (double)mats.cap) +
+           8.0 * ((double)red.cap + (double)gpart.cap + (double)gsum.cap);
   }
 
   void release() {
@@ -357,27 +388,31 @@ struct Workspace {
     stream = nullptr;
   }
 
-  // Tensor maps of a shape's passes over `base`.  Circuit shapes live for the
-  // whole batch and are cached by address; a job's private shape is encoded
-  // into `scratch` (its address may be reused by a later shape).
-  const std::vector<CUtensorMap>* maps_for(const Shape& s, double2* base, bool cache, std::vector<CUtensorMap>& scratch,
-                                           std::string& err) {
+  // Tensor maps of a shape's passes over `nsets` arrays at `base`.  Circuit
+  // shapes live for the whole call and are cached; a job's private shape is
+  // encoded into `scratch` (its address may be reused by a later shape).
+  const std::vector<CUtensorMap>* maps_for(const Shape& s, double2* base, uint32_t nsets, bool cache,
+                                           std::vector<CUtensorMap>& scratch, std::string& err) {
+    const auto key = std::make_pair(&s, nsets);
     if (cache) {
-      auto it = tmaps.find(&s);
+      auto it = tmaps.find(key);
       if (it != tmaps.end()) return &it->second;
     }
     std::vector<CUtensorMap> v(s.plans.size());
     char emsg[256];
-    for (size_t i = 0; i < s.plans.size(); ++i)
-      if (encode_pass_tmap(&v[i], base, s.nbits, s.plans[i].desc, emsg, sizeof(emsg)) != 0) {
+    for (size_t i = 0; i < s.plans.size(); ++i) {
+      PassDesc d = s.plans[i].desc;
+      d.nsets = nsets;
+      if (encode_pass_tmap(&v[i], base, s.nbits, d, emsg, sizeof(emsg)) != 0) {
         err = emsg;
         return nullptr;
       }
+    }
     if (!cache) {
       scratch = std::move(v);
       return &scratch;
     }
-    return &tmaps.emplace(&s, std::move(v)).first->second;
+    return &tmaps.emplace(key, std::move(v)).first->second;
   }
 };
 
@@ -387,30 +422,51 @@ bool cuda_ok(cudaError_t e, const char* what, std::string& err) {
   return false;
 }
 
-// launch a shape's passes on `state` (matrices at `mats`)
-bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double2* state, const double2* mats,
-               double* gpart, Stats& st, std::string& err) {
+int log2_u64(uint64_t x) {
+  int r = 0;
+  while ((1ULL << r) < x) ++r;
+  return r;
+}
+
+// Launch a shape's passes over `nsets` arrays of 2^nbits amplitudes at `state`
+// (set s's matrices at mats + s * mat_stride; gradient rows per set:
+// grad_stride).  Returns the tile-pass grid of the launches in *grid.
+bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double2* state, uint32_t nsets,
+               const double2* mats, uint32_t mat_stride, double* gpart, uint32_t grad_stride, unsigned* grid,
+               Stats& st, std::string& err) {
+  const uint64_t dim = 1ULL << s.nbits;
   if (!s.tiled) {
-    for (const SimpleOp& so : s.sops)
-      if (!cuda_ok(launch_simple_op(state, s.nbits, so, mats, w.stream), "gate kernel", err)) return false;
-    st.launches += s.sops.size();
-    st.bytes += (uint64_t)s.sops.size() * (32ULL << s.nbits);
+    for (uint32_t k = 0; k < nsets; ++k)
+      for (const SimpleOp& so : s.sops)
+        if (!cuda_ok(launch_simple_op(state + k * dim, s.nbits, so, mats + (size_t)k * mat_stride, w.stream),
+                     "gate kernel", err))
+          return false;
+    st.launches += s.sops.size() * nsets;
+    st.bytes += (uint64_t)s.sops.size() * nsets * (32ULL << s.nbits);
     return true;
   }
   std::vector<CUtensorMap> scratch;
-  const std::vector<CUtensorMap>* tm = w.maps_for(s, state, cached, scratch, err);
+  const std::vector<CUtensorMap>* tm = w.maps_for(s, state, nsets, cached, scratch, err);
   if (!tm) return false;
-  for (size_t i = 0; i < s.plans.size(); ++i)
-    if (!cuda_ok(launch_tile_pass((*tm)[i], s.plans[i].desc, mats, w.status.p, cfg.tl, w.num_sms, w.stream, gpart),
+  for (size_t i = 0; i < s.plans.size(); ++i) {
+    PassDesc d = s.plans[i].desc;
+    d.set_shift = (uint32_t)log2_u64(d.ntiles);
+    d.ntiles *= nsets;
+    d.nsets = nsets;
+    d.set_mat_stride = mat_stride;
+    d.grad_stride = grad_stride;
+    if (grid) *grid = tile_pass_grid(d, cfg.tl, w.num_sms);
+    if (!cuda_ok(launch_tile_pass((*tm)[i], d, mats, w.status.p, cfg.tl, w.num_sms, w.stream, gpart),
                  "tile pass kernel", err))
       return false;
+  }
   st.launches += s.plans.size();
-  st.bytes += (uint64_t)s.plans.size() * (32ULL << s.nbits);
+  st.bytes += (uint64_t)s.plans.size() * nsets * (32ULL << s.nbits);
   return true;
 }
 
 // Finish the job that used staging slot `k`: wait for its stream, check the
-// status word, write energy and gradient.
+// status word, write energies and gradients.
 bool finish(Workspace& w, int k, std::string& err) {
   Pending& p = w.pend[k];
   if (!p.active) return true;
@@ -427,58 +483,28 @@ bool finish(Workspace& w, int k, std::string& err) {
     return false;
   }
   Circuit& c = *p.c;
-  if (c.energy_out) c.energy_out[p.set] = out[0];
-  if (p.grad && c.grad_out) {
-    double* g = c.grad_out + p.set * (size_t)c.nparams;
-    for (int i = 0; i < c.nparams; ++i) g[i] = 0.0;
-    for (int t = 0; t < p.ngrads; ++t) g[p.grad_param[t]] += out[1 + t];
+  const size_t S = p.sets.size();
+  for (size_t j = 0; j < S; ++j) {
+    const size_t set = p.sets[j];
+    if (c.energy_out) c.energy_out[set] = out[j];
+    if (p.grad && c.grad_out) {
+      double* g = c.grad_out + set * (size_t)c.nparams;
+      for (int i = 0; i < c.nparams; ++i) g[i] = 0.0;
+      const double* row = out + S + j * (size_t)p.ngrads;
+      for (int t = 0; t < p.ngrads; ++t) g[p.grad_param[t]] += row[t];
+    }
   }
   return true;
 }
 
-// Prepare and launch one job on the workspace's stream.  want_grad = false:
-// forward and energy only.
-bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set, bool want_grad, Stats& st, std::string& err) {
-  const auto t0 = std::chrono::steady_clock::now();
-  const double* theta = c.params + set * (size_t)c.nparams;
-  JobOps j;
-  job_ops(cfg, c, theta, want_grad, j);
-  {
-    std::lock_guard<std::mutex> g(c.mu);
-    if (!c.planned) {
-      c.planned = true;
-      c.fw.reset(new Shape);
-      if (!make_shape(cfg, c.n, j.fw, j.fpool.size(), w.num_sms, *c.fw, c.plan_err)) c.fw.reset();
-      if (c.fw && want_grad) {
-        c.bw.reset(new Shape);
-        if (!make_shape(cfg, joint_bits(c.n), j.bw, j.bpool.size(), w.num_sms, *c.bw, c.plan_err)) c.bw.reset();
-        else c.bw->ngrads = (int)j.grad_param.size();
-      }
-    }
-    if (!c.fw || (want_grad && !c.bw)) {
-      err = "scheduler: " + c.plan_err;
-      return false;
-    }
-  }
-  // shapes for this set (the circuit's, or private ones if the structure differs)
-  std::unique_ptr<Shape> own_fw, own_bw;
-  const Shape* fw = c.fw.get();
-  const Shape* bw = c.bw.get();
-  if (!matches(*fw, j.fw, j.fpool.size())) {
-    own_fw.reset(new Shape);
-    if (!make_shape(cfg, c.n, j.fw, j.fpool.size(), w.num_sms, *own_fw, err)) return false;
-    fw = own_fw.get();
-    ++st.replans;
-  }
-  if (want_grad && !matches(*bw, j.bw, j.bpool.size())) {
-    own_bw.reset(new Shape);
-    if (!make_shape(cfg, joint_bits(c.n), j.bw, j.bpool.size(), w.num_sms, *own_bw, err)) return false;
-    own_bw->ngrads = (int)j.grad_param.size();
-    bw = own_bw.get();
-    ++st.replans;
-  }
-  const int ngrads = want_grad ? (int)j.grad_param.size() : 0;
-
+// Launch the parameter sets `sets` of circuit c together on the workspace's
+// stream, all through the shapes fw / bw (their fused operation lists match
+// every set's).  want_grad = false: forward and energy only.
+bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<size_t>& sets, std::vector<JobOps>& jo,
+                 const Shape* fw, bool fw_cached, const Shape* bw, bool bw_cached, bool want_grad, Stats& st,
+                 std::string& err, std::chrono::steady_clock::time_point t0) {
+  const uint32_t S = (uint32_t)sets.size();
+  const int ngrads = want_grad ? (int)jo[0].grad_param.size() : 0;
   // staging slot: wait for the job that used it last
   const int k = w.slot;
   w.slot ^= 1;
@@ -486,18 +512,34 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set, bool want_
   if (!finish(w, k, err)) return false;
   const auto tw1 = std::chrono::steady_clock::now();
   const size_t nf = fw->gather.size(), nb = want_grad ? bw->gather.size() : 0;
-  if (!w.hmats[k].ensure(nf + nb, err) || !w.hout[k].ensure(1 + (size_t)ngrads, err) || !w.hstat[k].ensure(1, err))
+  const size_t per = nf + nb;
+  if (!w.hmats[k].ensure(per * S, err) || !w.hout[k].ensure(S + (size_t)S * ngrads, err) || !w.hstat[k].ensure(1, err))
     return false;
   double2* hm = w.hmats[k].p;
-  for (size_t i = 0; i < nf; ++i) hm[i] = make_double2(j.fpool[fw->gather[i]].re, j.fpool[fw->gather[i]].im);
-  for (size_t i = 0; i < nb; ++i) hm[nf + i] = make_double2(j.bpool[bw->gather[i]].re, j.bpool[bw->gather[i]].im);
-
-  // device buffers (a buffer that grows waits for the stream's earlier work first)
-  if (!w.mats.ensure(2 * (nf + nb), err, "matrices", w.stream)) return false;
-  if (want_grad &&
-      (!w.gpart.ensure((size_t)std::max(ngrads, 1) * std::max(bw->grid, 1u), err, "gradient partials", w.stream) ||
-       !w.gsum.ensure((size_t)std::max(ngrads, 1), err, "gradient sums", w.stream)))
+  for (uint32_t j = 0; j < S; ++j) {
+    const JobOps& o = jo[j];
+    double2* f = hm + (size_t)j * nf;
+    for (size_t i = 0; i < nf; ++i) f[i] = make_double2(o.fpool[fw->gather[i]].re, o.fpool[fw->gather[i]].im);
+    double2* b = hm + (size_t)S * nf + (size_t)j * nb;
+    for (size_t i = 0; i < nb; ++i) b[i] = make_double2(o.bpool[bw->gather[i]].re, o.bpool[bw->gather[i]].im);
+  }
+  const uint64_t dim = 1ULL << c.n;
+  const int nj = joint_bits(c.n);
+  const uint64_t jdim = 1ULL << nj;
+  // device buffers (a buffer that grows waits for the stream's earlier work first);
+  // tensor maps hold the state buffers' addresses, so they are dropped if one moves
+  const double2* psi0 = w.psi.p;
+  const double2* joint0 = w.joint.p;
+  if (!w.mats.ensure(2 * per * S, err, "matrices", w.stream) ||
+      !w.red.ensure((size_t)S * (kRedBlocks + 1), err, "reduction partials", w.stream) ||
+      !w.psi.ensure(dim * S, err, "the states", w.stream))
     return false;
+  const unsigned max_grid = (unsigned)w.num_sms * (unsigned)std::max(1, cfg.tl.ctas_per_sm);
+  if (want_grad && (!w.joint.ensure(jdim * S, err, "the joint arrays", w.stream) ||
+                    !w.gpart.ensure((size_t)std::max(ngrads, 1) * S * max_grid, err, "gradient partials", w.stream) ||
+                    !w.gsum.ensure((size_t)std::max(ngrads, 1) * S, err, "gradient sums", w.stream)))
+    return false;
+  if (w.psi.p != psi0 || w.joint.p != joint0) w.tmaps.clear();
   if (w.ham_of != &c) {
     if (!w.zmask.ensure(c.ham.zmask.size(), err, "Hamiltonian", w.stream) ||
         !w.coef.ensure(c.ham.coef.size(), err, "Hamiltonian", w.stream))
@@ -511,61 +553,127 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set, bool want_
     w.ham_of = &c;
   }
   // matrices go to the half of the device buffer this slot owns, so the copy for
-  // job j+1 cannot overwrite matrices job j's passes still read
+  // the next job cannot overwrite matrices this job's passes still read
   double2* dm = w.mats.p + (size_t)k * (w.mats.cap / 2);
-  if (!cuda_ok(cudaMemcpyAsync(dm, hm, (nf + nb) * sizeof(double2), cudaMemcpyHostToDevice, w.stream), "H2D matrices",
+  if (!cuda_ok(cudaMemcpyAsync(dm, hm, per * S * sizeof(double2), cudaMemcpyHostToDevice, w.stream), "H2D matrices",
                err))
     return false;
   st.host_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                     (std::chrono::steady_clock::now() - t0) - (tw1 - tw))
-                     .count();
+                    (std::chrono::steady_clock::now() - t0) - (tw1 - tw))
+                    .count();
 
-  // forward from |0>
-  const uint64_t dim = 1ULL << c.n;
-  if (!cuda_ok(launch_set_basis(w.psi.p, dim, w.stream), "reset", err)) return false;
-  if (!run_shape(w, cfg, *fw, !own_fw, w.psi.p, dm, nullptr, st, err)) return false;
-  st.fw_passes += fw->tiled ? fw->plans.size() : fw->sops.size();
-  double* energy_dev = w.red.p + kRedBlocks;
+  // forward from |0> for every set
+  if (!cuda_ok(launch_set_basis_sets(w.psi.p, dim, (int)S, w.stream), "reset", err)) return false;
+  if (!run_shape(w, cfg, *fw, fw_cached, w.psi.p, S, dm, (uint32_t)nf, nullptr, 0, nullptr, st, err)) return false;
+  st.fw_passes += (fw->tiled ? fw->plans.size() : fw->sops.size()) * S;
+  double* partials = w.red.p;
+  double* energy_dev = w.red.p + (size_t)S * kRedBlocks;
   if (!want_grad) {
-    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, c.ham.groups, w.zmask.p, w.coef.p, nullptr, w.red.p,
-                                          energy_dev, w.stream),
+    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, (int)S, 0, c.ham.groups, w.zmask.p, w.coef.p, nullptr,
+                                          partials, energy_dev, w.stream),
                  "energy kernel", err))
       return false;
     st.launches += 3;
   } else {
-    const int nj = joint_bits(c.n);
-    if (nj > c.n + 1 &&
-        !cuda_ok(cudaMemsetAsync(w.joint.p + 2 * dim, 0, ((1ULL << nj) - 2 * dim) * sizeof(double2), w.stream),
-                 "memset", err))
-      return false;
-    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, c.ham.groups, w.zmask.p, w.coef.p, w.joint.p, w.red.p,
-                                          energy_dev, w.stream),
+    if (nj > c.n + 1)
+      for (uint32_t j = 0; j < S; ++j)
+        if (!cuda_ok(cudaMemsetAsync(w.joint.p + j * jdim + 2 * dim, 0, (jdim - 2 * dim) * sizeof(double2), w.stream),
+                     "memset", err))
+          return false;
+    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, (int)S, jdim, c.ham.groups, w.zmask.p, w.coef.p, w.joint.p,
+                                          partials, energy_dev, w.stream),
                  "Hamiltonian kernel", err))
       return false;
-    if (!run_shape(w, cfg, *bw, !own_bw, w.joint.p, dm + nf, w.gpart.p, st, err)) return false;
-    st.bw_passes += bw->tiled ? bw->plans.size() : bw->sops.size();
-    if (!cuda_ok(launch_row_sums(w.gpart.p, ngrads, (int)bw->grid, w.gsum.p, w.stream), "gradient sums", err))
+    unsigned grid = 0;
+    // partials of the sets a CTA never reaches stay zero
+    if (ngrads && !cuda_ok(cudaMemsetAsync(w.gpart.p, 0, (size_t)ngrads * S * max_grid * sizeof(double), w.stream),
+                           "memset", err))
       return false;
-    st.launches += 4;
+    if (!run_shape(w, cfg, *bw, bw_cached, w.joint.p, S, dm + (size_t)S * nf, (uint32_t)nb, w.gpart.p,
+                   (uint32_t)ngrads, &grid, st, err))
+      return false;
+    st.bw_passes += (bw->tiled ? bw->plans.size() : bw->sops.size()) * S;
+    if (ngrads && grid == 0) { err = "internal: no gradient pass"; return false; }
+    if (!cuda_ok(launch_row_sums(w.gpart.p, ngrads * (int)S, (int)grid, w.gsum.p, w.stream), "gradient sums", err))
+      return false;
+    st.launches += 5;
   }
-  st.bytes += 16ULL * dim + (want_grad ? 32ULL * dim : 0);   // read psi; write the joint array
+  st.bytes += S * (16ULL * dim + (want_grad ? 32ULL * dim : 0));   // read psi; write the joint arrays
   double* ho = w.hout[k].p;
-  if (!cuda_ok(cudaMemcpyAsync(ho, energy_dev, sizeof(double), cudaMemcpyDeviceToHost, w.stream), "D2H", err) ||
+  if (!cuda_ok(cudaMemcpyAsync(ho, energy_dev, S * sizeof(double), cudaMemcpyDeviceToHost, w.stream), "D2H", err) ||
       !cuda_ok(cudaMemcpyAsync(w.hstat[k].p, w.status.p, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H", err))
     return false;
-  if (ngrads &&
-      !cuda_ok(cudaMemcpyAsync(ho + 1, w.gsum.p, (size_t)ngrads * sizeof(double), cudaMemcpyDeviceToHost, w.stream),
-               "D2H", err))
+  if (ngrads && !cuda_ok(cudaMemcpyAsync(ho + S, w.gsum.p, (size_t)S * ngrads * sizeof(double), cudaMemcpyDeviceToHost,
+                                         w.stream),
+                         "D2H", err))
     return false;
   if (!cuda_ok(cudaEventRecord(w.ev[k], w.stream), "event", err)) return false;
   Pending& p = w.pend[k];
   p.active = true;
   p.c = &c;
-  p.set = set;
+  p.sets = sets;
   p.grad = want_grad;
   p.ngrads = ngrads;
-  p.grad_param = std::move(j.grad_param);
-  ++st.jobs;
+  p.grad_param = want_grad ? jo[0].grad_param : std::vector<int>();
+  st.jobs += S;
+  return true;
+}
+
+// Prepare and launch the parameter sets [set0, set0 + nsets) of circuit c:
+// the sets whose fused operation lists match the circuit's plans run together;
+// any other set runs alone with plans of its own.
+bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set0, size_t nsets, bool want_grad, Stats& st,
+                std::string& err) {
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<JobOps> jo(nsets);
+  for (size_t j = 0; j < nsets; ++j) job_ops(cfg, c, c.params + (set0 + j) * (size_t)c.nparams, want_grad, jo[j]);
+  {
+    std::lock_guard<std::mutex> g(c.mu);
+    if (!c.planned) {
+      c.planned = true;
+      c.fw.reset(new Shape);
+      if (!make_shape(cfg, c.n, jo[0].fw, jo[0].fpool.size(), w.num_sms, *c.fw, c.plan_err)) c.fw.reset();
+      if (c.fw && want_grad) {
+        c.bw.reset(new Shape);
+        if (!make_shape(cfg, joint_bits(c.n), jo[0].bw, jo[0].bpool.size(), w.num_sms, *c.bw, c.plan_err)) c.bw.reset();
+        else c.bw->ngrads = (int)jo[0].grad_param.size();
+      }
+    }
+    if (!c.fw || (want_grad && !c.bw)) {
+      err = "scheduler: " + c.plan_err;
+      return false;
+    }
+  }
+  std::vector<size_t> same, other;
+  std::vector<JobOps> jsame;
+  for (size_t j = 0; j < nsets; ++j) {
+    const bool ok = matches(*c.fw, jo[j].fw, jo[j].fpool.size()) &&
+                    (!want_grad || matches(*c.bw, jo[j].bw, jo[j].bpool.size()));
+    if (ok) {
+      same.push_back(set0 + j);
+      jsame.push_back(std::move(jo[j]));
+    } else {
+      other.push_back(j);
+    }
+  }
+  if (!same.empty() &&
+      !launch_sets(w, cfg, c, same, jsame, c.fw.get(), true, c.bw.get(), true, want_grad, st, err, t0))
+    return false;
+  for (size_t j : other) {   // a set whose angles change the fused structure
+    const auto t1 = std::chrono::steady_clock::now();
+    std::unique_ptr<Shape> own_fw(new Shape), own_bw;
+    if (!make_shape(cfg, c.n, jo[j].fw, jo[j].fpool.size(), w.num_sms, *own_fw, err)) return false;
+    if (want_grad) {
+      own_bw.reset(new Shape);
+      if (!make_shape(cfg, joint_bits(c.n), jo[j].bw, jo[j].bpool.size(), w.num_sms, *own_bw, err)) return false;
+      own_bw->ngrads = (int)jo[j].grad_param.size();
+    }
+    ++st.replans;
+    std::vector<JobOps> one(1);
+    one[0] = std::move(jo[j]);
+    if (!launch_sets(w, cfg, c, {set0 + j}, one, own_fw.get(), false, own_bw.get(), false, want_grad, st, err, t1))
+      return false;
+  }
   return true;
 }
 
@@ -586,6 +694,36 @@ int current_device(std::string& err) {
 
 thread_local double t_stats[8] = {0};
 
+// Workspaces kept between calls (streams, events and buffers are costly to
+// create and allocation synchronises the device).  A workspace holding more
+// than kPoolKeepBytes of device memory is freed at the end of its call;
+// iq_adjoint_release frees the rest.  Never freed at process exit.
+constexpr double kPoolKeepBytes = 8.0 * (1ull << 30);
+std::mutex g_pool_mu;
+std::vector<Workspace*>* g_pool = new std::vector<Workspace*>();
+
+Workspace* pool_take(int dev) {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  for (size_t i = 0; i < g_pool->size(); ++i)
+    if ((*g_pool)[i]->device == dev) {
+      Workspace* w = (*g_pool)[i];
+      g_pool->erase(g_pool->begin() + i);
+      return w;
+    }
+  return new Workspace();
+}
+
+void pool_give(Workspace* w, bool ok) {
+  if (!ok || w->device_bytes() > kPoolKeepBytes) {
+    w->release();
+    delete w;
+    return;
+  }
+  cudaStreamSynchronize(w->stream);
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  g_pool->push_back(w);
+}
+
 // Run all jobs of `circs` (every parameter set of every circuit) on `nstreams` workers.
 int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool want_grad) {
   const auto t0 = std::chrono::steady_clock::now();
@@ -595,21 +733,38 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const Cfg cfg = Cfg::from_env();
-  struct Job { Circuit* c; size_t set; double cost; };
+  // jobs: a circuit's parameter sets in groups whose states (psi: 16 B x 2^n,
+  // joint: 32 B x 2^n per set) fit the per-job budget; the energy-only path
+  // (the plain baseline) runs one set per job
+  struct Job { Circuit* c; size_t set0, nsets; double cost; };
   std::vector<Job> jobs;
-  int nmax = 1;
+  const double job_bytes = env_double("IQ_ADJOINT_JOB_BYTES", 4.0 * (1ull << 30));
+  Workspace::Bounds bd;
   for (auto& c : circs) {
-    nmax = std::max(nmax, c->n);
-    for (size_t s = 0; s < c->nsets; ++s)
-      jobs.push_back({c.get(), s, std::ldexp((double)c->ops.size() + 1.0, c->n)});
+    const double per_set = 48.0 * std::ldexp(1.0, c->n);
+    const size_t group = want_grad ? (size_t)std::max(1.0, std::floor(job_bytes / per_set)) : 1;
+    // per set: at most 3 rotations per gate, each at most a dense 4x4 (16
+    // elements) forward and one backward; at most 3 gradient terms per gate
+    const size_t nops = c->ops.size() + 1;
+    for (size_t s0 = 0; s0 < c->nsets; s0 += group) {
+      const size_t ns = std::min(group, c->nsets - s0);
+      jobs.push_back({c.get(), s0, ns, (double)ns * std::ldexp((double)nops, c->n)});
+      bd.psi_amps = std::max<uint64_t>(bd.psi_amps, (uint64_t)ns << c->n);
+      if (want_grad) bd.joint_amps = std::max<uint64_t>(bd.joint_amps, (uint64_t)ns << joint_bits(c->n));
+      bd.mats = std::max(bd.mats, ns * 96 * nops);
+      bd.sets = std::max(bd.sets, ns);
+      if (want_grad) bd.grads = std::max(bd.grads, ns * 3 * nops);
+    }
   }
   if (jobs.empty()) return 0;
-  // largest first; sets of one circuit stay together so the first plans for the rest
+  // largest first
   std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) { return a.cost > b.cost; });
   // workers: as asked, no more than jobs, and as many workspaces as fit in 80% of free memory
   size_t freeb = 0, totalb = 0;
   cudaMemGetInfo(&freeb, &totalb);
-  const double per = 16.0 * (std::ldexp(1.0, nmax) + std::ldexp(1.0, joint_bits(nmax))) + (64 << 20);
+  const int max_grid = sms * std::max(1, cfg.tl.ctas_per_sm);
+  const double per = 16.0 * ((double)bd.psi_amps + (double)bd.joint_amps) + 16.0 * (double)bd.mats +
+                     8.0 * (double)bd.grads * (max_grid + 2) / 3.0 + (64 << 20);
   int nw = nstreams > 0 ? nstreams : env_int("IQ_ADJOINT_STREAMS", 8);
   nw = std::min<int>(nw, (int)jobs.size());
   nw = std::min<int>(nw, std::max(1, (int)(0.8 * (double)freeb / per)));
@@ -621,13 +776,14 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   std::string first_err;
   auto worker = [&](int id) {
     (void)id;
-    Workspace w;
+    Workspace* wp = pool_take(dev);
+    Workspace& w = *wp;
     std::string e;
-    bool ok = w.init(dev, sms, nmax, e);
+    bool ok = w.prepare(dev, sms, bd, e);
     while (ok) {
       const size_t i = next.fetch_add(1);
       if (i >= jobs.size()) break;
-      ok = launch_job(w, cfg, *jobs[i].c, jobs[i].set, want_grad, st, e);
+      ok = launch_job(w, cfg, *jobs[i].c, jobs[i].set0, jobs[i].nsets, want_grad, st, e);
       std::lock_guard<std::mutex> g(emu);
       if (!first_err.empty()) ok = false;   // another worker failed: stop taking jobs
     }
@@ -637,7 +793,7 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
       std::lock_guard<std::mutex> g(emu);
       if (first_err.empty()) first_err = e.empty() ? "adjoint worker failed" : e;
     }
-    w.release();
+    pool_give(wp, ok);
   };
   if (nw == 1) {
     worker(0);
@@ -735,6 +891,20 @@ int iq_adjoint_gradient_batch(const iq_adjoint_circuit* circuits, size_t num_cir
 }
 
 int iq_ansatz_energy(const iq_adjoint_circuit* circuit) { return run_circuits(circuit, 1, 1, false); }
+
+int iq_adjoint_release(void) {
+  std::vector<Workspace*> ws;
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    ws.swap(*g_pool);
+  }
+  for (Workspace* w : ws) {
+    cudaSetDevice(w->device);
+    w->release();
+    delete w;
+  }
+  return (int)ws.size();
+}
 
 int iq_adjoint_stats(double* out, size_t n) {
   if (!out) return -1;

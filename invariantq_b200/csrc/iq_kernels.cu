@@ -409,6 +409,18 @@ cudaError_t launch_set_basis(double2* s, uint64_t dim, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// nsets arrays of dim (a power of two) amplitudes end to end, each set to e_0
+__global__ void set_basis_sets_kernel(double2* __restrict__ s, uint64_t dim, uint64_t total) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x)
+    s[i] = make_double2((i & (dim - 1)) == 0 ? 1.0 : 0.0, 0.0);
+}
+
+cudaError_t launch_set_basis_sets(double2* s, uint64_t dim, int nsets, cudaStream_t st) {
+  const uint64_t total = dim * (uint64_t)(nsets < 1 ? 1 : nsets);
+  set_basis_sets_kernel<<<grid_for(total, 256), 256, 0, st>>>(s, dim, total);
+  return cudaGetLastError();
+}
+
 __global__ void split_kernel(const double2* __restrict__ s, uint64_t n, double* __restrict__ re, double* __restrict__ im) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const double2 a = s[i];
@@ -564,9 +576,15 @@ cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, i
 // Re conj(psi) lambda.
 // H = sum over groups g of sum over terms t of c_t (-1)^popc((x ^ xmask_g) & zmask_t)
 // psi[x ^ xmask_g]: Pauli strings sharing their X part share one gather.
+__global__ void row_sum_kernel(const double* __restrict__ in, int cols, double* __restrict__ out);
+
+// blockIdx.y = set: psi + set * dim, joint + set * jdim, partials + set * gridDim.x
 __global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64_t dim, HamTerms h,
                                          const uint64_t* __restrict__ zmask, const double2* __restrict__ coef,
-                                         double2* __restrict__ joint, double* __restrict__ partials) {
+                                         double2* __restrict__ joint, uint64_t jdim, double* __restrict__ partials) {
+  psi += blockIdx.y * dim;
+  if (joint) joint += blockIdx.y * jdim;
+  partials += (size_t)blockIdx.y * gridDim.x;
   double e = 0.0;
   for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
     const double2 px = psi[x];
@@ -592,11 +610,13 @@ __global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64
   if (threadIdx.x == 0) partials[blockIdx.x] = e;
 }
 
-cudaError_t launch_hamiltonian_joint(const double2* psi, int n, const HamTerms& h, const uint64_t* zmask,
-                                     const double2* coef, double2* joint, double* partials, double* energy,
-                                     cudaStream_t st) {
-  hamiltonian_joint_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(psi, 1ULL << n, h, zmask, coef, joint, partials);
-  final_sum_kernel<<<1, 1024, 0, st>>>(partials, kRedBlocks, energy);
+cudaError_t launch_hamiltonian_joint(const double2* psi, int n, int nsets, uint64_t jdim, const HamTerms& h,
+                                     const uint64_t* zmask, const double2* coef, double2* joint, double* partials,
+                                     double* energy, cudaStream_t st) {
+  if (nsets < 1) nsets = 1;
+  hamiltonian_joint_kernel<<<dim3(kRedBlocks, nsets), kRedThreads, 0, st>>>(psi, 1ULL << n, h, zmask, coef, joint,
+                                                                            jdim, partials);
+  row_sum_kernel<<<nsets, 256, 0, st>>>(partials, kRedBlocks, energy);
   return cudaGetLastError();
 }
 

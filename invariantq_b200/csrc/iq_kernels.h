@@ -75,6 +75,8 @@ cudaError_t launch_collapse(double2* s, uint64_t dim, uint64_t mask, uint64_t va
 // rho[r][c] *= factor if bits(r) and bits(c) at mask both equal val, else 0
 cudaError_t launch_dm_collapse(double2* rho, int n, uint64_t mask, uint64_t val, double factor, cudaStream_t st);
 cudaError_t launch_set_basis(double2* s, uint64_t dim, cudaStream_t st);   // s = e_0
+// nsets arrays of dim amplitudes (dim a power of two) laid end to end, each set to e_0
+cudaError_t launch_set_basis_sets(double2* s, uint64_t dim, int nsets, cudaStream_t st);
 cudaError_t launch_split(const double2* s, uint64_t count, double* re, double* im, cudaStream_t st);
 cudaError_t launch_probs(const double2* s, uint64_t count, double* p, cudaStream_t st);
 
@@ -98,11 +100,12 @@ struct HamTerms {
   uint64_t xmask[kMaxHamGroups];
   int first[kMaxHamGroups + 1];
 };
-// joint[2x] = psi[x], joint[2x+1] = (H psi)[x] for x < 2^n (when joint is not null);
-// *energy = Re <psi|H|psi>
-cudaError_t launch_hamiltonian_joint(const double2* psi, int n, const HamTerms& h, const uint64_t* zmask,
-                                     const double2* coef, double2* joint, double* partials, double* energy,
-                                     cudaStream_t st);
+// For each of nsets states psi_s = psi + s * 2^n: joint_s[2x] = psi_s[x],
+// joint_s[2x+1] = (H psi_s)[x] with joint_s = joint + s * jdim (when joint is
+// not null), and energy[s] = Re <psi_s|H|psi_s>.  partials: nsets * kRedBlocks.
+cudaError_t launch_hamiltonian_joint(const double2* psi, int n, int nsets, uint64_t jdim, const HamTerms& h,
+                                     const uint64_t* zmask, const double2* coef, double2* joint, double* partials,
+                                     double* energy, cudaStream_t st);
 cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st);
 
 // Record an error for iq_last_error (defined in iq_runtime.cu).

@@ -85,6 +85,16 @@ struct PassDesc {
   uint32_t mat_elems;            // complex elements in the block (ops' `mat` are relative to it)
   uint32_t grad_base;            // gradient term index of the pass's first OP_GRAD2
   uint32_t ngrad;                // OP_GRAD2 terms in the pass (consecutive indices, <= kMaxPassGrads)
+  // Several arrays of 2^nbits amplitudes laid end to end ("sets", e.g. one per
+  // parameter set of a circuit), all run through the same planned operations
+  // with their own matrices: ntiles counts the tiles of every set, set s owns
+  // tiles [s << set_shift, (s + 1) << set_shift), its matrix block starts
+  // set_mat_stride complex elements after set s - 1's, and its gradient terms
+  // are rows s * grad_stride + gidx of the partials.  nsets 0 or 1: one array.
+  uint32_t nsets;
+  uint32_t set_shift;
+  uint32_t set_mat_stride;
+  uint32_t grad_stride;
   StageDesc st[kMaxStages];
   OpDesc ops[kMaxPassOps];
 };
@@ -167,18 +177,19 @@ IQ_HD void pass_tmap_layout(const PassDesc& d, int nbits, uint64_t gd[5], uint64
   gs[0] = 8 * E;
   box[0] = 16;
   box[1] = 1u << (c - 3);
+  const uint64_t sets = d.nsets > 1 ? d.nsets : 1;   // sets extend the top dimension
   if (d.nbox == 2) {
     const int h0 = d.H[0], h1 = d.H[1];
-    gd[1] = 1ull << (h0 - 3); gd[2] = 2; gd[3] = 1ull << (h1 - h0 - 1); gd[4] = 1ull << (nbits - h1);
+    gd[1] = 1ull << (h0 - 3); gd[2] = 2; gd[3] = 1ull << (h1 - h0 - 1); gd[4] = (1ull << (nbits - h1)) * sets;
     gs[1] = (1ull << h0) * E; gs[2] = (1ull << (h0 + 1)) * E; gs[3] = (1ull << h1) * E;
     box[2] = 2; box[3] = 1; box[4] = 2;
   } else if (d.nbox == 1) {
     const int h0 = d.H[0];
-    gd[1] = 1ull << (h0 - 3); gd[2] = 1ull << (nbits - h0); gd[3] = 1; gd[4] = 1;
+    gd[1] = 1ull << (h0 - 3); gd[2] = (1ull << (nbits - h0)) * sets; gd[3] = 1; gd[4] = 1;
     gs[1] = (1ull << h0) * E; gs[2] = top; gs[3] = top;
     box[2] = 2; box[3] = 1; box[4] = 1;
   } else {
-    gd[1] = 1ull << (nbits - 3); gd[2] = 1; gd[3] = 1; gd[4] = 1;
+    gd[1] = (1ull << (nbits - 3)) * sets; gd[2] = 1; gd[3] = 1; gd[4] = 1;
     gs[1] = top; gs[2] = top; gs[3] = top;
     box[2] = 1; box[3] = 1; box[4] = 1;
   }

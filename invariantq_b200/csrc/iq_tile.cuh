@@ -674,9 +674,24 @@ __global__ void __launch_bounds__(NT, MINB)
   const int lane = tid & 31;
   const uint32_t tile_elems = 1u << P.M;
   double2* smat = tiles + (size_t)nbuf * tile_elems;
-  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + i];
+  const uint64_t ntiles = P.ntiles;
+  const uint64_t first = blockIdx.x;
+  // set of the tiles being processed (the CTA's tiles ascend, so each set is
+  // met in one run); its matrices sit in smat, its gradient sums in gslots
+  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
+  uint32_t cur_set = (first < ntiles) ? (uint32_t)(first >> sshift) : 0u;
+  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + i];
   double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
   for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
+  // gradient partials of the current set: octet rows summed in order, one
+  // column per CTA; rows the CTA never touches stay as the host zeroed them
+  auto flush_grads = [&]() {
+    for (uint32_t i = tid; i < P.ngrad; i += NT) {
+      double v = 0.0;
+      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
+      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_base + i) * gridDim.x + blockIdx.x] = v;
+    }
+  };
   if (tid == 0) {
     for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
     abort_flag = 0;
@@ -684,8 +699,6 @@ __global__ void __launch_bounds__(NT, MINB)
   }
   __syncthreads();
 
-  const uint64_t ntiles = P.ntiles;
-  const uint64_t first = blockIdx.x;
   const uint64_t cnt = (first < ntiles) ? (ntiles - 1 - first) / gridDim.x + 1 : 0;
   const int depth = nbuf >= 3 ? nbuf - 2 : nbuf - 1;   // < nbuf
 
@@ -766,6 +779,18 @@ __global__ void __launch_bounds__(NT, MINB)
     const bool ok = bounded_wait(&bar_loaded[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status, DEV_WAIT_LOADED);
     const bool work = __syncthreads_and(ok && !abort_flag);
     if (!work && first_unwaited == cnt) first_unwaited = i;
+    const uint32_t tset = (uint32_t)((first + i * gridDim.x) >> sshift);   // uniform in the CTA
+    if (tset != cur_set) {   // every thread is past the previous tile's stages
+      if (P.ngrad) {
+        flush_grads();
+        __syncthreads();
+        for (uint32_t j = tid; j < P.ngrad * (NT / 8); j += NT) gslots[j] = 0.0;
+      }
+      cur_set = tset;
+      for (uint32_t j = tid; j < P.mat_elems; j += NT)
+        smat[j] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + j];
+      __syncthreads();
+    }
     double2* buf = tiles + (size_t)b * tile_elems;
     for (int s = 0; s < P.nstages; ++s) {
       if (work) run_stage<R>(buf, P, s, smat, tid, NT, gslots);
@@ -778,13 +803,9 @@ __global__ void __launch_bounds__(NT, MINB)
   // after an abort, let loads that were issued but never consumed land first
   for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
   bulk_wait_all();
-  if (P.ngrad) {   // one column of per-CTA partials per gradient term, octet rows summed in order
+  if (P.ngrad) {   // the last set's gradient partials
     __syncthreads();
-    for (uint32_t i = tid; i < P.ngrad; i += NT) {
-      double v = 0.0;
-      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
-      grad_partials[(size_t)(P.grad_base + i) * gridDim.x + blockIdx.x] = v;
-    }
+    flush_grads();
   }
 }
 

@@ -184,6 +184,11 @@ def parameter_shift_gradient(ansatz: Ansatz, ham: PauliHamiltonian, params) -> n
     return 0.5 * (e[0::2] - e[1::2])
 
 
+def adjoint_release() -> int:
+    """Free the workspaces the adjoint calls keep between calls."""
+    return int(_lib.load().iq_adjoint_release())
+
+
 def adjoint_stats() -> dict:
     """Counters of this thread's last adjoint / energy call."""
     lib = _lib.load()

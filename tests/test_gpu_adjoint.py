@@ -76,8 +76,10 @@ def test_large_gradient_vs_gpu_parameter_shift(G, n, layers):
 
 
 def test_batch_matches_single_jobs(G):
-    """Uneven circuits and several parameter sets on several streams give the
-    same numbers as one job at a time (same plans, fixed reduction order)."""
+    """Uneven circuits, several parameter sets each (run together in one launch
+    per pass), on several streams: bit-identical for any number of streams (fixed
+    reduction order), equal to one set at a time within 1e-13 (the sets' tiles
+    meet the CTAs in another order), and to the parameter shift within 1e-9."""
     rng = np.random.default_rng(9)
     jobs = []
     for n, L in [(4, 2), (10, 3), (13, 2), (7, 4), (12, 1)]:
@@ -86,12 +88,31 @@ def test_batch_matches_single_jobs(G):
     out = G.adjoint_gradient_batch(jobs, num_streams=4)
     st = G.adjoint_stats()
     assert st["jobs"] == 15 and st["streams"] == 4
+    out1 = G.adjoint_gradient_batch(jobs, num_streams=1)
+    for (e, g), (e1, g1) in zip(out, out1):
+        assert np.array_equal(e, e1) and np.array_equal(g, g1)
     for (a, h, P), (e, g) in zip(jobs, out):
         for s in range(P.shape[0]):
             e1, g1 = G.adjoint_gradient(a, h, P[s])
             assert e[s] == e1
-            assert np.array_equal(g[s], g1)
+            assert np.max(np.abs(g[s] - g1)) < 1e-13
             assert np.max(np.abs(g[s] - G.parameter_shift_gradient(a, h, P[s]))) < PS_TOL
+
+
+def test_batched_sets_at_scale(G):
+    """16 parameter sets of a 16-qubit circuit in one batched job against
+    each set alone (multi-tile passes, set boundaries inside CTAs' tile runs);
+    then the kept workspaces are released and a call after that still works."""
+    a, h = G.Ansatz.hardware_efficient(16, 3), G.PauliHamiltonian.tfim(16, 1.0)
+    P = np.random.default_rng(13).uniform(0, 2 * np.pi, (16, a.num_params))
+    (e, g), = G.adjoint_gradient_batch([(a, h, P)], num_streams=1)
+    for s in (0, 7, 15):
+        e1, g1 = G.adjoint_gradient(a, h, P[s])
+        assert abs(e[s] - e1) < 1e-13
+        assert np.max(np.abs(g[s] - g1)) < 1e-12
+    assert G.adjoint_release() >= 1
+    e2, g2 = G.adjoint_gradient(a, h, P[7])
+    assert abs(e2 - e[7]) < 1e-13 and np.max(np.abs(g2 - g[7])) < 1e-12
 
 
 def test_structure_change_across_sets_is_replanned(G, port):
