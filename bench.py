@@ -274,8 +274,9 @@ def adjoint_section(args, rank, world):
     one-circuit-at-a-time parameter-shift path on a sample of the same circuits."""
     import torch
     from invariantq_b200.gradients import adjoint_gradient_batch, adjoint_stats, parameter_shift_gradient
+    from invariantq_b200.replicas import max_over_ranks, shard
     jobs = gradient_jobs(args.adjoint_circuits, args.adjoint_sets)
-    mine = jobs[rank::world]
+    mine = shard(jobs, rank, world)
     grads = sum(P.shape[0] for _, _, P in mine)
     partials = sum(P.shape[0] * P.shape[1] for _, _, P in mine)
     adjoint_gradient_batch(mine, args.adjoint_streams)            # warm-up (allocations, first plans)
@@ -285,11 +286,7 @@ def adjoint_section(args, rank, world):
         out = adjoint_gradient_batch(mine, args.adjoint_streams)
         times.append(time.perf_counter() - t0)
     st = adjoint_stats()
-    t = float(np.median(times))
-    if world > 1:
-        x = torch.tensor([t], dtype=torch.float64, device=f"cuda:{int(os.environ.get('LOCAL_RANK', 0))}")
-        torch.distributed.all_reduce(x, op=torch.distributed.ReduceOp.MAX)
-        t = float(x.item())
+    t = max_over_ranks(float(np.median(times)), device=f"cuda:{int(os.environ.get('LOCAL_RANK', 0))}")
     # parameter-shift baseline on every k-th circuit of this rank (first parameter set)
     ps_t, ps_n, err = 0.0, 0, 0.0
     for i in range(0, len(mine), max(args.ps_stride, 1)):
@@ -555,6 +552,7 @@ def our_arm(args, rank, world, local_rank):
     from invariantq_b200 import _lib
     from invariantq_b200.binding import NativeStateVector
     from invariantq_b200.simulator import apply_gate_matrix
+    from invariantq_b200.replicas import max_over_ranks
 
     dist = world > 1
     lib = _lib.load()
@@ -605,10 +603,7 @@ def our_arm(args, rank, world, local_rank):
     clk = clocks.stop() if clocks else None
     pass_ms = sv.profile_read()
     sv.set_option("profile", 0)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, device=f"cuda:{local_rank}")
 
     # e2e through the reference-facing C ABI (host matrices every step, <Z_i> read back)
     e2e = None
@@ -627,10 +622,7 @@ def our_arm(args, rank, world, local_rank):
                 e2e_times.append(dt)
         h2d = (sv.stats()["h2d_bytes"] - h2d0) / args.steps
         e2e_ms = sum(e2e_times) / len(e2e_times) * 1e3
-        if dist:
-            t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, device=f"cuda:{local_rank}")
         e2e = {"value": round(world * prog.passes * pass_bytes(n) / (e2e_ms / 1e3) / 1e9, 3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * n + 4),
                "ms_per_step": round(e2e_ms, 3)}
@@ -688,10 +680,9 @@ def our_arm(args, rank, world, local_rank):
 
 
 def main():
+    from invariantq_b200.replicas import env_ranks
     args = parse()
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    rank, world, local_rank = env_ranks()
     if args.impl == "reference":
         reference_arm(args, rank)
         return
