@@ -520,7 +520,8 @@ def density_matrix_section(args):
 def adjoint30_section(args):
     """One 30-qubit adjoint gradient: 16 layers of RY and RZ on every qubit
     plus a CZ ring (960 parameters), TFIM H with h = 0.7, complex128; the
-    gradient is checked against the parameter-shift rule on 4 parameters."""
+    gradient is checked against the parameter-shift rule on 4 parameters.  The
+    same gradient again with complex64 states, and its error against complex128."""
     from invariantq_b200.gradients import Ansatz, PauliHamiltonian, adjoint_gradient, adjoint_stats, ansatz_energies
     from invariantq_b200.gradients import shifted_parameter_sets
     n, L = 30, 16
@@ -537,12 +538,20 @@ def adjoint30_section(args):
     rows = np.concatenate([[2 * j, 2 * j + 1] for j in idx])
     es = ansatz_energies(a, h, sets[rows])
     ps = 0.5 * (es[0::2] - es[1::2])
+    from invariantq_b200.gradients import adjoint_gradient_c64
+    t0 = time.perf_counter()
+    e32, g32 = adjoint_gradient_c64(a, h, th)
+    t32 = time.perf_counter() - t0
     return {"workload": f"{n}q, {L} layers RY+RZ per qubit + CZ ring ({a.num_params} parameters), TFIM h=0.7, complex128; "
                         "three state-sized buffers (psi and the 2^(n+1) psi/lambda array), no checkpoints",
             "gradient_s": round(t, 3), "energy": e, "passes": {"forward": int(st["forward_passes"]),
                                                               "backward": int(st["backward_passes"])},
             "achieved_gbs": round(st["bytes"] / t / 1e9, 1),
-            "max_abs_diff_vs_param_shift": float(np.max(np.abs(ps - g[idx]))), "checked_parameters": [int(i) for i in idx]}
+            "max_abs_diff_vs_param_shift": float(np.max(np.abs(ps - g[idx]))), "checked_parameters": [int(i) for i in idx],
+            "complex64": {"gradient_s": round(t32, 3), "energy_abs_err": abs(e32 - e),
+                          "grad_max_abs_err": float(np.max(np.abs(g32 - g))),
+                          "grad_rel_err": float(np.max(np.abs(g32 - g)) / max(np.max(np.abs(g)), 1e-300)),
+                          "states": "psi and lambda as complex64 (2 x 8 GiB), FP64 arithmetic and sums"}}
 
 
 # ---------------------------------------------------------------- our arm

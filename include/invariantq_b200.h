@@ -223,6 +223,16 @@ typedef struct iq_adjoint_circuit {
 int iq_adjoint_gradient(size_t num_qubits, size_t num_ops, const int* kinds, const int* q0, const int* q1,
                         const int* param_index, size_t num_params, const double* params, size_t num_terms,
                         const double* coeffs, const char* paulis, double* energy_out, double* grad_out);
+/* The same gradient with the states stored as complex64 (8 B per amplitude,
+ * half the memory and traffic of complex128): every gate and Hamiltonian
+ * product is computed in FP64 from the loaded amplitudes and rounded once on
+ * store, every sum (gradient terms, energy) is accumulated in FP64.  One
+ * parameter set; two state buffers (psi and lambda, 8 B x 2^n each).  The
+ * result differs from iq_adjoint_gradient by the complex64 rounding of the
+ * states (~1e-7 relative at 30 qubits, 16 layers). */
+int iq_adjoint_gradient_c64(size_t num_qubits, size_t num_ops, const int* kinds, const int* q0, const int* q1,
+                            const int* param_index, size_t num_params, const double* params, size_t num_terms,
+                            const double* coeffs, const char* paulis, double* energy_out, double* grad_out);
 /* Every parameter set of every circuit, run concurrently on num_streams CUDA
  * streams (<= 0: IQ_ADJOINT_STREAMS or 8), each with its own device workspace;
  * the parameter sets of one circuit run together, through the same tile-pass

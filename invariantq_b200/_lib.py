@@ -111,6 +111,8 @@ SIGNATURES = {
     "iq_adjoint_gradient": ([_sz, _sz, c_ip, c_ip, c_ip, c_ip, _sz, c_dp, _sz, c_dp, ctypes.c_char_p, c_dp, c_dp],
                             _i),
     "iq_adjoint_gradient_batch": ([ctypes.POINTER(AdjointCircuit), _sz, _i], _i),
+    "iq_adjoint_gradient_c64": ([_sz, _sz, c_ip, c_ip, c_ip, c_ip, _sz, c_dp, _sz, c_dp, ctypes.c_char_p, c_dp, c_dp],
+                                _i),
     "iq_ansatz_energy": ([ctypes.POINTER(AdjointCircuit)], _i),
     "iq_adjoint_stats": ([c_dp, _sz], _i),
     "iq_adjoint_release": ([], _i),

@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "../../include/invariantq_b200.h"
+#include "iq_c64.h"
 #include "iq_kernels.h"
 #include "iq_plan.h"
 
@@ -861,6 +862,219 @@ int run_circuits(const iq_adjoint_circuit* in, size_t count, int nstreams, bool 
   return run_batch(circs, nstreams, want_grad);
 }
 
+// ------------------------------------------------------------ complex64 variant
+//
+// The same gradient with amplitudes stored as complex64 (float2) and FP64
+// arithmetic and reductions (iq_c64.cu).  The ansatz becomes items: runs of
+// one-qubit gates on one qubit (at most kC64MaxRunOps, flushed before any
+// two-qubit gate on that qubit; gates on different qubits commute, so the
+// circuit is unchanged) and CZ / CX gates.  Forward: one pass per item (a run
+// applies its product matrix).  Backward, items in reverse: a run records each
+// rotation's Im<lambda|P|psi> and un-applies it, last gate first, in one pass
+// over psi and lambda.
+
+struct C64Item {
+  int kind;        // 0 = run, 1 = CZ, 2 = CX (a = control, b = target)
+  int a, b;
+  C64Run run;
+  C64Mat fwd;      // the run's product matrix
+};
+
+void mat_rot(int gen, double c, double s, double* m) {   // exp(-i t P / 2), re/im interleaved
+  for (int i = 0; i < 8; ++i) m[i] = 0.0;
+  if (gen == 0) { m[0] = c; m[3] = -s; m[5] = -s; m[6] = c; }
+  else if (gen == 1) { m[0] = c; m[2] = -s; m[4] = s; m[6] = c; }
+  else { m[0] = c; m[1] = -s; m[6] = c; m[7] = s; }
+}
+
+void mat_mul(const double* a, const double* b, double* o) {   // o = a b
+  double t[8];
+  for (int r = 0; r < 2; ++r)
+    for (int cc = 0; cc < 2; ++cc) {
+      double re = 0.0, im = 0.0;
+      for (int k = 0; k < 2; ++k) {
+        const double ar = a[2 * (2 * r + k)], ai = a[2 * (2 * r + k) + 1];
+        const double br = b[2 * (2 * k + cc)], bi = b[2 * (2 * k + cc) + 1];
+        re += ar * br - ai * bi;
+        im += ar * bi + ai * br;
+      }
+      t[2 * (2 * r + cc)] = re;
+      t[2 * (2 * r + cc) + 1] = im;
+    }
+  for (int i = 0; i < 8; ++i) o[i] = t[i];
+}
+
+void mat_dagger(const double* m, double* o) {
+  double t[8];
+  for (int r = 0; r < 2; ++r)
+    for (int cc = 0; cc < 2; ++cc) {
+      t[2 * (2 * r + cc)] = m[2 * (2 * cc + r)];
+      t[2 * (2 * r + cc) + 1] = -m[2 * (2 * cc + r) + 1];
+    }
+  for (int i = 0; i < 8; ++i) o[i] = t[i];
+}
+
+void mat_fixed(int kind, double* m) {   // H, X, SX
+  for (int i = 0; i < 8; ++i) m[i] = 0.0;
+  const double r = 1.0 / std::sqrt(2.0);
+  if (kind == GATE_H) { m[0] = r; m[2] = r; m[4] = r; m[6] = -r; }
+  else if (kind == GATE_X) { m[2] = 1.0; m[4] = 1.0; }
+  else { m[0] = 0.5; m[1] = 0.5; m[2] = 0.5; m[3] = -0.5; m[4] = 0.5; m[5] = -0.5; m[6] = 0.5; m[7] = 0.5; }
+}
+
+void build_c64_items(int n, const std::vector<AnsatzOp>& ops, const double* theta, std::vector<C64Item>& items,
+                     std::vector<int>& term_param) {
+  std::vector<C64Item> open(n);
+  for (int q = 0; q < n; ++q) {
+    open[q].kind = 0;
+    open[q].run.q = q;
+    open[q].run.nops = 0;
+  }
+  auto reset = [&](int q) {
+    open[q].run.nops = 0;
+    double* f = open[q].fwd.m;
+    for (int i = 0; i < 8; ++i) f[i] = 0.0;
+    f[0] = f[6] = 1.0;
+  };
+  for (int q = 0; q < n; ++q) reset(q);
+  auto flush = [&](int q) {
+    if (open[q].run.nops) items.push_back(open[q]);
+    reset(q);
+  };
+  auto push = [&](int q, const C64Op& o, const double* fwd) {
+    if (open[q].run.nops == kC64MaxRunOps) flush(q);
+    open[q].run.ops[open[q].run.nops++] = o;
+    mat_mul(fwd, open[q].fwd.m, open[q].fwd.m);
+  };
+  auto rot = [&](int q, int gen, int par) {
+    C64Op o{};
+    o.gen = gen;
+    o.term = (int)term_param.size();
+    term_param.push_back(par);
+    o.c = std::cos(0.5 * theta[par]);
+    o.s = std::sin(0.5 * theta[par]);
+    double f[8];
+    mat_rot(gen, o.c, o.s, f);
+    push(q, o, f);
+  };
+  for (const AnsatzOp& a : ops) {
+    switch (a.kind) {
+      case GATE_RX: rot(a.q0, 0, a.param); break;
+      case GATE_RY: rot(a.q0, 1, a.param); break;
+      case GATE_RZ: case GATE_P: rot(a.q0, 2, a.param); break;   // P = phase x Rz
+      case GATE_U3:   // e^{i(phi+lambda)/2} Rz(phi) Ry(theta) Rz(lambda)
+        rot(a.q0, 2, a.param + 2);
+        rot(a.q0, 1, a.param);
+        rot(a.q0, 2, a.param + 1);
+        break;
+      case GATE_H: case GATE_X: case GATE_SX: {
+        C64Op o{};
+        o.gen = -1;
+        double f[8];
+        mat_fixed(a.kind, f);
+        mat_dagger(f, o.inv);
+        push(a.q0, o, f);
+        break;
+      }
+      default: {   // CZ, CX
+        flush(a.q0);
+        flush(a.q1);
+        C64Item it{};
+        it.kind = a.kind == GATE_CZ ? 1 : 2;
+        it.a = a.q0;
+        it.b = a.q1;
+        items.push_back(it);
+      }
+    }
+  }
+  for (int q = 0; q < n; ++q) flush(q);
+}
+
+int adjoint_c64(const iq_adjoint_circuit& in) {
+  Circuit c;
+  std::string err;
+  if (!load_circuit(in, c, true, err)) { record_error(E_ARG, err.c_str()); return -1; }
+  if (in.num_sets != 1) { record_error(E_ARG, "the complex64 variant takes one parameter set"); return -1; }
+  const int dev = current_device(err);
+  if (dev < 0) { record_error(E_DEVICE, err.c_str()); return -1; }
+  std::vector<C64Item> items;
+  std::vector<int> term_param;
+  build_c64_items(c.n, c.ops, c.params, items, term_param);
+  const int T = (int)term_param.size();
+  const uint64_t dim = 1ULL << c.n;
+  float2 *psi = nullptr, *lam = nullptr;
+  double *partials = nullptr, *sums = nullptr;
+  uint64_t* zm = nullptr;
+  double2* co = nullptr;
+  cudaStream_t st = nullptr;
+  uint64_t launches = 0;
+  bool ok = true;
+  auto check = [&](cudaError_t e, const char* what) {
+    if (ok && e != cudaSuccess) {
+      ok = false;
+      err = std::string(what) + ": " + cudaGetErrorString(e);
+    }
+    return ok;
+  };
+  check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+  if (ok && (cudaMalloc(&psi, dim * sizeof(float2)) != cudaSuccess ||
+             cudaMalloc(&lam, dim * sizeof(float2)) != cudaSuccess)) {
+    cudaGetLastError();
+    ok = false;
+    err = "cannot allocate device memory for the complex64 states";
+  }
+  check(cudaMalloc(&partials, ((size_t)T + 1) * kC64Blocks * sizeof(double)), "cudaMalloc partials");
+  check(cudaMalloc(&sums, ((size_t)T + 1) * sizeof(double)), "cudaMalloc sums");
+  check(cudaMalloc(&zm, c.ham.zmask.size() * 8), "cudaMalloc Hamiltonian");
+  check(cudaMalloc(&co, c.ham.coef.size() * 16), "cudaMalloc Hamiltonian");
+  check(cudaMemcpyAsync(zm, c.ham.zmask.data(), c.ham.zmask.size() * 8, cudaMemcpyHostToDevice, st), "H2D");
+  check(cudaMemcpyAsync(co, c.ham.coef.data(), c.ham.coef.size() * 16, cudaMemcpyHostToDevice, st), "H2D");
+  check(c64_set_basis(psi, c.n, st), "reset");
+  ++launches;
+  for (const C64Item& it : items) {   // forward
+    if (!ok) break;
+    if (it.kind == 0) check(c64_apply1q(psi, c.n, it.run.q, it.fwd, st), "complex64 gate kernel");
+    else if (it.kind == 1) check(c64_cz(psi, c.n, it.a, it.b, st), "complex64 CZ kernel");
+    else check(c64_cx(psi, c.n, it.a, it.b, st), "complex64 CX kernel");
+    ++launches;
+  }
+  double* hpart = partials + (size_t)T * kC64Blocks;
+  check(c64_hamiltonian(psi, c.n, c.ham.groups, zm, co, lam, hpart, st), "complex64 Hamiltonian kernel");
+  ++launches;
+  for (size_t i = items.size(); ok && i-- > 0;) {   // backward
+    const C64Item& it = items[i];
+    if (it.kind == 0) {
+      check(c64_grad_run(psi, lam, c.n, it.run, partials, st), "complex64 adjoint kernel");
+      ++launches;
+    } else {
+      for (float2* s2 : {psi, lam}) {
+        if (it.kind == 1) check(c64_cz(s2, c.n, it.a, it.b, st), "complex64 CZ kernel");
+        else check(c64_cx(s2, c.n, it.a, it.b, st), "complex64 CX kernel");
+        ++launches;
+      }
+    }
+  }
+  if (ok) check(launch_row_sums(partials, T + 1, kC64Blocks, sums, st), "sums");
+  launches += 1;
+  std::vector<double> h((size_t)T + 1);
+  if (ok) check(cudaMemcpyAsync(h.data(), sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+  if (st) check(cudaStreamSynchronize(st), "stream sync");
+  for (void* p : {(void*)psi, (void*)lam, (void*)partials, (void*)sums, (void*)zm, (void*)co})
+    if (p) cudaFree(p);
+  if (st) cudaStreamDestroy(st);
+  count_launches(launches);
+  if (!ok) {
+    record_error(E_CUDA, err.c_str());
+    return -1;
+  }
+  if (c.energy_out) c.energy_out[0] = h[T];
+  if (c.grad_out) {
+    for (int i = 0; i < c.nparams; ++i) c.grad_out[i] = 0.0;
+    for (int t = 0; t < T; ++t) c.grad_out[term_param[t]] += h[t];
+  }
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -884,6 +1098,27 @@ int iq_adjoint_gradient(size_t num_qubits, size_t num_ops, const int* kinds, con
   c.energy_out = energy_out;
   c.grad_out = grad_out;
   return run_circuits(&c, 1, 1, true);
+}
+
+int iq_adjoint_gradient_c64(size_t num_qubits, size_t num_ops, const int* kinds, const int* q0, const int* q1,
+                            const int* param_index, size_t num_params, const double* params, size_t num_terms,
+                            const double* coeffs, const char* paulis, double* energy_out, double* grad_out) {
+  iq_adjoint_circuit c{};
+  c.num_qubits = num_qubits;
+  c.num_ops = num_ops;
+  c.kinds = kinds;
+  c.q0 = q0;
+  c.q1 = q1;
+  c.param_index = param_index;
+  c.num_params = num_params;
+  c.num_sets = 1;
+  c.params = params;
+  c.num_terms = num_terms;
+  c.coeffs = coeffs;
+  c.paulis = paulis;
+  c.energy_out = energy_out;
+  c.grad_out = grad_out;
+  return adjoint_c64(c);
 }
 
 int iq_adjoint_gradient_batch(const iq_adjoint_circuit* circuits, size_t num_circuits, int num_streams) {
