@@ -89,10 +89,19 @@ def apply_gate_matrix(sv: NativeStateVector, qubits: List[int], matrix: np.ndarr
 
 
 class StateVectorSimulator:
-    def __init__(self, max_memory_bytes: Optional[int] = None, entropy_max_side: int = 10):
+    """``autotune``: None / False (default settings), True (an
+    ``autotune.Autotuner`` with its default cache) or an ``Autotuner``; the
+    chosen fusion width and tile-pass settings are applied and their choice ID
+    is reported in ``metadata["autotune"]``."""
+
+    def __init__(self, max_memory_bytes: Optional[int] = None, entropy_max_side: int = 10, autotune=None):
         self.name = "statevector"
         self.max_memory_bytes = max_memory_bytes
         self.entropy_max_side = entropy_max_side
+        if autotune is True:
+            from .autotune import Autotuner
+            autotune = Autotuner()
+        self.autotuner = autotune or None
 
     def run(self, circuit, shots: int = 1024, seed: int = 42, *, allow_non_unitary: bool = False,
             execution_context=None, return_statevector: bool = True) -> ExecutionResult:
@@ -108,11 +117,21 @@ class StateVectorSimulator:
         if self.max_memory_bytes is not None and mem_bytes > self.max_memory_bytes:
             raise MemoryError(f"statevector requires approximately {mem_bytes} bytes including a working copy, "
                               f"above configured limit {self.max_memory_bytes}")
+        tuned = None
+        if self.autotuner is not None:
+            tuned = self.autotuner.choose(circuit)
+            if tuned["k"] > 2:
+                from .fusion import GateFusionPass
+                circuit = GateFusionPass(tuned["k"]).run(circuit)
         ctx = execution_context
         if ctx is not None:
             ctx.__enter__()
         try:
             sv = NativeStateVector(n)
+            if tuned is not None:
+                for key in ("tile_bits", "budget", "reg_slots"):
+                    sv.set_option(key, tuned[key])
+            sv.set_option("profile", 1)
             for op in circuit.ops:
                 if ctx is not None:
                     ctx.check()
@@ -148,6 +167,7 @@ class StateVectorSimulator:
             if ctx is not None:
                 ctx.check()
             stats = sv.stats()
+            kernel_ms = float(np.sum(sv.profile_read(1 << 20)))
         finally:
             if ctx is not None:
                 ctx.__exit__(None, None, None)
@@ -158,6 +178,13 @@ class StateVectorSimulator:
             memory_used_bytes=mem_bytes, shots=shots,
             metadata={"num_qubits": n, "dimension": 1 << n, "allow_non_unitary": allow_non_unitary,
                       "state_norm": float(np.sum(probs_vec)), "core": native_core_status(), "gpu": stats,
+                      "gate_passes": int(stats["passes"]), "bytes_moved": float(stats["bytes"]),
+                      "kernel_ms": kernel_ms,
+                      "achieved_GBps": (float(stats["bytes"]) / kernel_ms / 1e6) if kernel_ms > 0 else None,
+                      "autotune": None if tuned is None else {
+                          "choice_id": tuned["choice_id"], "cached": tuned["cached"], "k": tuned["k"],
+                          "tile_bits": tuned["tile_bits"], "budget": tuned["budget"],
+                          "reg_slots": tuned["reg_slots"]},
                       "provenance": {"requested_backend": self.name, "selected_backend": "statevector",
                                      "implementation": "dense_statevector", "native": True,
                                      "exact": not allow_non_unitary, "resource_limit_bytes": self.max_memory_bytes,
