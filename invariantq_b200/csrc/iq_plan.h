@@ -63,7 +63,7 @@ struct OpDesc {          // 16 bytes
   uint8_t flags;
   uint8_t pad0, pad1;
   uint32_t mat;          // offset (complex elements) into the flush's matrix buffer
-  uint32_t gidx;         // OP_GRAD2: gradient term index (global; see PassDesc::grad_base)
+  uint32_t gidx;         // OP_GRAD2: the pass's local gradient index (global term: PassDesc::grad_term)
 };
 
 struct StageDesc {       // 28 bytes
@@ -83,14 +83,15 @@ struct PassDesc {
   uint32_t nops, pad2;
   uint32_t mat_base;             // this pass's matrix block in the flush's matrix pool
   uint32_t mat_elems;            // complex elements in the block (ops' `mat` are relative to it)
-  uint32_t grad_base;            // gradient term index of the pass's first OP_GRAD2
-  uint32_t ngrad;                // OP_GRAD2 terms in the pass (consecutive indices, <= kMaxPassGrads)
+  uint32_t grad_base;            // unused (0)
+  uint32_t ngrad;                // OP_GRAD2 steps in the pass (<= kMaxPassGrads)
+  uint32_t grad_term[kMaxPassGrads];   // global gradient term of local index i
   // Several arrays of 2^nbits amplitudes laid end to end ("sets", e.g. one per
   // parameter set of a circuit), all run through the same planned operations
   // with their own matrices: ntiles counts the tiles of every set, set s owns
   // tiles [s << set_shift, (s + 1) << set_shift), its matrix block starts
   // set_mat_stride complex elements after set s - 1's, and its gradient terms
-  // are rows s * grad_stride + gidx of the partials.  nsets 0 or 1: one array.
+  // are rows s * grad_stride + term of the partials.  nsets 0 or 1: one array.
   uint32_t nsets;
   uint32_t set_shift;
   uint32_t set_mat_stride;
@@ -307,7 +308,7 @@ void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* param
 // an adjoint step (gradient term + inverse rotation) per rotation angle, or the
 // inverse of a fixed gate.  grad_param[t] is the parameter gradient term t adds to.
 void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                     std::vector<cplx64>& pool, std::vector<int>& grad_param);
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit = 0);
 // Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
 // and fills perm/phases/unit if every row and column holds exactly one nonzero.
 int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);

@@ -87,6 +87,14 @@ struct PassBuilder {
     for (int i = 0; i < s.nS; ++i) n += s.S[i] < c;
     return n;
   }
+  // Chunk bits a stage may hold in slots: c - 3 keeps three chunk bits free for
+  // lane operations.  A stage without lane operations may take one more: its
+  // lanes can then use the first tile bit above the chunk, whose swizzled
+  // image also has a low bit set, so the octet's accesses can stay on eight
+  // bank groups (the lane choice below takes the best rank it finds).
+  int lowlimit(const Stage& s, bool no_lanes_after) const {
+    return c - kLaneBits + ((no_lanes_after && s.lanereq == 0) ? 1 : 0);
+  }
   // Register slots take at most c - 3 of the chunk bits [0, c), so three lane
   // bits always remain inside the chunk; lane operations name up to 3 of them.
   bool tryAdd(Stage& s, const SchedOp& op) const {
@@ -95,7 +103,7 @@ struct PassBuilder {
       const int b = op.q[0];
       const uint64_t bm = 1ULL << b;
       if (inS(s, b) || (s.lanereq & bm)) return true;
-      if (b < c && __builtin_popcountll(s.lanereq) < kLaneBits) {
+      if (b < c && __builtin_popcountll(s.lanereq) < kLaneBits && lowcount(s) <= c - kLaneBits) {
         s.lanereq |= bm;
         return true;
       }
@@ -108,7 +116,7 @@ struct PassBuilder {
     for (int i = 0; i < 2; ++i)
       if (!inS(s, op.q[i])) { need[nn++] = op.q[i]; lowadd += op.q[i] < c; }
     if (s.nS + nn > p.R) return false;
-    if (lowcount(s) + lowadd > c - kLaneBits) return false;
+    if (lowcount(s) + lowadd > lowlimit(s, op.grad != 0)) return false;
     for (int i = 0; i < nn; ++i) {
       s.S[s.nS++] = need[i];
       s.lanereq &= ~(1ULL << need[i]);   // earlier lane ops on this bit become slot ops
@@ -233,25 +241,36 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     if (o.k > p.R) { err = "dense block wider than the register slots"; return -1; }
   }
 
-  // per-bit queues of op indices (dependency order)
+  // per-bit queues of op indices (dependency order).  An adjoint step applies
+  // the same 2x2 to the psi and lambda halves and never mixes them, so steps on
+  // different qubits commute (their gradient terms too: Im<lambda|P_b|psi> does
+  // not change when a unitary on another qubit acts on both halves); when no
+  // other operation touches the select bit, adjoint steps are ordered by their
+  // qubit bit only.
+  std::vector<uint8_t> other_use(nb, 0);
+  for (int i = 0; i < nops; ++i)
+    if (!ops[i].grad)
+      for (int j = 0; j < ops[i].k; ++j) other_use[ops[i].q[j]] = 1;
+  auto dep_first = [&](int i) { return (ops[i].grad && !other_use[ops[i].q[0]]) ? 1 : 0; };
+  auto ndeps = [&](int i) { return ops[i].k - dep_first(i); };
   std::vector<std::vector<int>> q(nb);
   std::vector<size_t> head(nb, 0);
   for (int i = 0; i < nops; ++i)
-    for (int j = 0; j < ops[i].k; ++j) q[ops[i].q[j]].push_back(i);
+    for (int j = dep_first(i); j < ops[i].k; ++j) q[ops[i].q[j]].push_back(i);
   std::vector<int> headcnt(nops, 0);
   std::set<int> ready;
   for (int b = 0; b < nb; ++b)
     if (!q[b].empty()) {
       int i = q[b][0];
-      if (++headcnt[i] == ops[i].k) ready.insert(i);
+      if (++headcnt[i] == ndeps(i)) ready.insert(i);
     }
   auto retire = [&](int i) {
-    for (int j = 0; j < ops[i].k; ++j) {
+    for (int j = dep_first(i); j < ops[i].k; ++j) {
       int b = ops[i].q[j];
       ++head[b];
       if (head[b] < q[b].size()) {
         int nx = q[b][head[b]];
-        if (++headcnt[nx] == ops[nx].k) ready.insert(nx);
+        if (++headcnt[nx] == ndeps(nx)) ready.insert(nx);
       }
     }
   };
@@ -330,6 +349,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     for (size_t i = 0; i < H.size(); ++i) d.H[i] = (uint8_t)H[i];
     d.ntiles = 1ULL << (nb - M);
     d.nstages = (uint8_t)pb.stages.size();
+    d.ngrad = 0;
     int nout = 0;
     for (size_t si = 0; si < pb.stages.size(); ++si) {
       const Stage& s = pb.stages[si];
@@ -391,7 +411,8 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
           if (o.grad) {
             od.perm = o.gen;
             od.flags = 0;
-            od.gidx = o.gidx;
+            od.gidx = d.ngrad;                 // local index; the global term goes to grad_term
+            d.grad_term[d.ngrad++] = o.gidx;
           }
         } else {
           for (int t = 0; t < o.k; ++t)
@@ -402,18 +423,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
       sd.op1 = (uint16_t)nout;
     }
     d.nops = (uint32_t)nout;
-    d.ngrad = 0;
     d.grad_base = 0;
-    for (int i : taken)
-      if (ops[i].grad) {
-        if (d.ngrad == 0 || ops[i].gidx < d.grad_base) d.grad_base = ops[i].gidx;
-        ++d.ngrad;
-      }
-    for (int i : taken)
-      if (ops[i].grad && (ops[i].gidx < d.grad_base || ops[i].gidx >= d.grad_base + d.ngrad)) {
-        err = "internal: gradient terms of a pass are not consecutive";
-        return -1;
-      }
     plan.nsrc = (int)taken.size();
     plan.cost = cost;
     out.push_back(plan);
@@ -722,8 +732,9 @@ void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* param
 }
 
 void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                     std::vector<cplx64>& pool, std::vector<int>& grad_param) {
-  (void)n;
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit) {
+  if (select_bit < 0) select_bit = n;
+  auto bit = [&](int q) { return q + (q >= select_bit ? 1 : 0); };   // index bit of qubit q in the joint array
   for (size_t i = ops.size(); i-- > 0;) {
     const AnsatzOp& o = ops[i];
     int gen[3], par[3];
@@ -735,8 +746,8 @@ void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* para
         dagger2(m, md);
         SchedOp g{};
         g.k = 2;
-        g.q[0] = 0;                       // psi / lambda select bit
-        g.q[1] = (uint8_t)(o.q0 + 1);
+        g.q[0] = (uint8_t)select_bit;     // psi / lambda select bit
+        g.q[1] = (uint8_t)bit(o.q0);
         g.grad = 1;
         g.gen = (uint8_t)gen[r];
         g.gidx = (uint32_t)grad_param.size();
@@ -753,7 +764,7 @@ void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* para
     const int d = 1 << k;
     for (int r = 0; r < d; ++r)
       for (int c = 0; c < d; ++c) md[r * d + c] = std::conj(m[c * d + r]);
-    int qj[2] = {q[0] + 1, q[1] + 1};
+    int qj[2] = {bit(q[0]), k > 1 ? bit(q[1]) : 0};
     push_op(out, pool, k, qj, md);
   }
 }

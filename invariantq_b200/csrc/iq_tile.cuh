@@ -537,6 +537,7 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
                                          const double2* mats, int lane8, unsigned omask, double2* tile,
                                          const uint32_t (&sb)[R], uint32_t base, double* sgrad,
                                          uint32_t grad_base) {
+  (void)grad_base;
   const double2* m = mats + od.mat;
   const bool unit = od.flags & OPF_UNIT_PHASE;
   switch (od.kind) {
@@ -546,7 +547,7 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
       if (od.perm == 0) acc = disp_grad2_b<R, 0>(od.b, s, d, m);
       else if (od.perm == 1) acc = disp_grad2_b<R, 1>(od.b, s, d, m);
       else acc = disp_grad2_b<R, 2>(od.b, s, d, m);
-      grad_accumulate(acc, sgrad + (od.gidx - grad_base), lane8, omask);
+      grad_accumulate(acc, sgrad + od.gidx, lane8, omask);
       break;
     }
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(NT, MINB)
     for (uint32_t i = tid; i < P.ngrad; i += NT) {
       double v = 0.0;
       for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
-      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_base + i) * gridDim.x + blockIdx.x] = v;
+      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_term[i]) * gridDim.x + blockIdx.x] = v;
     }
   };
   if (tid == 0) {

@@ -165,7 +165,8 @@ struct Emu {
             break;
           case OP_GRAD2: {
             if (od.a != 0) { err = "adjoint step with the select bit outside slot 0"; return false; }
-            if (od.gidx >= grads.size()) grads.resize(od.gidx + 1, 0.0);
+            const uint32_t term = P.grad_term[od.gidx];
+            if (term >= grads.size()) grads.resize(term + 1, 0.0);
             const int B = od.b;
             for (int L = 0; L < 8; ++L)
               for (int v = 0; v < NV; ++v) {
@@ -175,7 +176,7 @@ struct Emu {
                 if (od.perm == 0) t = std::conj(l0) * p1 + std::conj(l1) * p0;
                 else if (od.perm == 1) t = std::conj(l0) * (cd(0, -1) * p1) + std::conj(l1) * (cd(0, 1) * p0);
                 else t = std::conj(l0) * p0 - std::conj(l1) * p1;
-                grads[od.gidx] += t.imag();
+                grads[term] += t.imag();
                 a[L][v] = mat(od.mat, 0) * p0 + mat(od.mat, 1) * p1;
                 a[L][v | (1 << B)] = mat(od.mat, 2) * p0 + mat(od.mat, 3) * p1;
                 a[L][v | 1] = mat(od.mat, 0) * l0 + mat(od.mat, 1) * l1;
