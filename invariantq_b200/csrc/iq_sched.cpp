@@ -125,10 +125,26 @@ struct PassBuilder {
   }
   bool place(int idx, const SchedOp& op) {
     if (op.grad) {
-      // adjoint steps want the psi / lambda select bit in register slot 0
-      if (!stages.empty()) {
+      // adjoint steps want the psi / lambda select bit in register slot 0; slot
+      // positions bind to operations only when the pass is finalised, so the
+      // current stage can take the select bit into slot 0 (swapped there, or
+      // inserted when a slot is free and the chunk-bit limit allows)
+      if (!stages.empty() && !stages.back().dk) {
         Stage trial = stages.back();
-        if (!trial.dk && trial.nS > 0 && trial.S[0] == op.q[0] && tryAdd(trial, op)) {
+        const int sel = op.q[0];
+        bool ready = trial.nS > 0 && trial.S[0] == sel;
+        if (!ready && inS(trial, sel)) {
+          for (int i = 1; i < trial.nS; ++i)
+            if (trial.S[i] == sel) std::swap(trial.S[0], trial.S[i]);
+          ready = true;
+        } else if (!ready && trial.nS < p.R && !(trial.lanereq & (1ULL << sel)) &&
+                   (sel >= c || lowcount(trial) + 1 <= lowlimit(trial, true))) {
+          for (int i = trial.nS; i > 0; --i) trial.S[i] = trial.S[i - 1];
+          trial.S[0] = sel;
+          ++trial.nS;
+          ready = true;
+        }
+        if (ready && tryAdd(trial, op)) {
           trial.ops.push_back(idx);
           stages.back() = trial;
           return true;
