@@ -70,7 +70,9 @@ struct Cfg {
     c.sp.c = env_int("IQ_CHUNK_BITS", 5);
     c.sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
-    c.sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
+    // adjoint sweeps: a larger budget than the state-vector default (80) -- their
+    // passes are cheaper per operation (structured rotations, unit CZ phases)
+    c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 120.0));
     c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
     c.tl.nbuf = env_int("IQ_NBUF", 3);
     c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
