@@ -134,7 +134,8 @@ void* iq_statevector_device_ptr(void* sv);
 void* iq_statevector_stream(void* sv);
 size_t iq_statevector_num_qubits(void* sv);
 
-/* Tuning / diagnostics for either handle kind.  Keys: "tile_bits", "chunk_bits",
+/* Tuning / diagnostics for either handle kind ("inject_status" = code: set the
+ * handle's device status word, as a timed-out tile pass would).  Keys: "tile_bits", "chunk_bits",
  * "reg_slots" (register slots R = 3, 4, 5 per tile-pass thread: 2^R amplitudes
  * each; raised to the widest fused block), "max_stages", "budget", "nbuf",
  * "ctas_per_sm", "eager", "fuse", "flush_ops", "profile".  0 = ok, -1 =
@@ -253,6 +254,15 @@ int iq_ansatz_energy(const iq_adjoint_circuit* circuit);
  * HBM bytes of the passes, [5] host preparation ms (summed over workers),
  * [6] wall ms, [7] streams used.  Returns the number of counters (8). */
 int iq_adjoint_stats(double* out, size_t n);
+
+/* Failure-path check (no counterpart in the reference): one CTA waits, with
+ * the tile kernel's bounded wait, on an mbarrier phase that never completes.
+ * The wait gives up after limit_ms (at most 1000), sets the status word and the
+ * kernel returns, leaving the GPU context usable.  Returns the status the
+ * kernel set (1: a tile load timed out) and the time it waited in *waited_ms;
+ * -1 on a CUDA error.  Handles report the same status word on their next
+ * synchronising call (option "inject_status" sets it, for tests). */
+int iq_selftest_bounded_wait(double limit_ms, double* waited_ms);
 
 /* Density-matrix additions. */
 int iq_density_matrix_flush(void* dm);

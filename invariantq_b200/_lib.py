@@ -115,6 +115,7 @@ SIGNATURES = {
                                 _i),
     "iq_ansatz_energy": ([ctypes.POINTER(AdjointCircuit)], _i),
     "iq_adjoint_stats": ([c_dp, _sz], _i),
+    "iq_selftest_bounded_wait": ([_d, c_dp], _i),
     "iq_adjoint_release": ([], _i),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),

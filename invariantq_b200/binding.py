@@ -339,3 +339,16 @@ class NativeDensityMatrix(_Handle):
         p = self._lib.iq_density_matrix_device_ptr(self._ptr)
         check(self._lib)
         return p
+
+
+def selftest_bounded_wait(limit_ms: float = 20.0) -> tuple:
+    """Runs the tile kernel's bounded wait on an mbarrier that never completes
+    (iq_selftest_bounded_wait): returns (status, waited_ms).  Status 1 means the
+    wait gave up and reported a timed-out tile load, as it should."""
+    lib = _lib.load()
+    waited = ctypes.c_double()
+    st = lib.iq_selftest_bounded_wait(float(limit_ms), ctypes.byref(waited))
+    if st < 0:
+        check(lib)
+        raise RuntimeError("iq_selftest_bounded_wait failed")
+    return st, waited.value

@@ -1066,6 +1066,12 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "fuse")) e->fuse = iv ? 1 : 0;
   else if (!strcmp(key, "flush_ops")) { if (iv < 1) return -1; e->flush_ops = iv; }
   else if (!strcmp(key, "profile")) e->profile = iv ? 1 : 0;
+  else if (!strcmp(key, "inject_status")) {   // failure-path tests: as if a tile pass had timed out
+    if (iv < 1 || iv > 2) return -1;
+    if (!cuda_ok(cudaMemcpyAsync(e->d_status, &iv, sizeof(int), cudaMemcpyHostToDevice, e->stream), "inject status") ||
+        !cuda_ok(cudaStreamSynchronize(e->stream), "stream sync"))
+      return -1;
+  }
   else { set_error(E_ARG, "unknown option '%s'", key); return -1; }
   return 0;
 }

@@ -154,13 +154,13 @@ __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity) {
 // plus the status word) when the limit runs out, or as soon as another thread
 // of the CTA has aborted.
 __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                             int* status, int code) {
+                                             int* status, int code, uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   for (;;) {
     if (mbar_try_wait_suspend(bar, parity, kWaitSuspendNs)) return true;
     if (*abort_flag) return false;
-    if (global_ns() - t0 > kWaitLimitNs) break;
+    if (global_ns() - t0 > limit_ns) break;
   }
   *abort_flag = 1;
   atomicCAS(status, 0, code);

@@ -98,3 +98,41 @@ def test_shard_rejects_bad_rank():
         shard([1, 2, 3], 2, 2)
     assert shard(list(range(7)), 1, 3) == [1, 4]
     assert max_over_ranks(1.5) == 1.5    # no process group: the value itself
+
+
+def _leaving_rank(rank, world, port, out_dir):
+    """Rank 1 leaves after the first step (between steps: nothing of its own in
+    flight); rank 0 goes on to the next step's timing reduction, which must end
+    with an error, not wait for good."""
+    import time
+    import torch.distributed as dist
+    from invariantq_b200.replicas import max_over_ranks
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    first = max_over_ranks(1.0 + rank)
+    if rank == 1:
+        dist.destroy_process_group()
+        return
+    t0 = time.monotonic()
+    try:
+        max_over_ranks(3.0)
+        outcome = "completed"
+    except Exception as exc:                       # gloo: connection closed, or the group's timeout
+        outcome = type(exc).__name__
+    elapsed = time.monotonic() - t0
+    with open(os.path.join(out_dir, "leave.pkl"), "wb") as f:
+        pickle.dump((first, outcome, elapsed), f)
+    try:
+        dist.destroy_process_group()
+    except Exception:
+        pass
+
+
+def test_rank_leaving_ends_next_collective_with_error(tmp_path):
+    import torch.multiprocessing as mp
+    mp.start_processes(_leaving_rank, args=(2, free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    first, outcome, elapsed = pickle.loads((tmp_path / "leave.pkl").read_bytes())
+    assert first == 2.0                 # the step both ranks took
+    assert outcome != "completed"
+    assert elapsed < 30.0               # bounded by the 5 s group timeout (plus teardown)
