@@ -138,15 +138,27 @@ size_t iq_statevector_num_qubits(void* sv);
  * handle's device status word, as a timed-out tile pass would).  Keys: "tile_bits", "chunk_bits",
  * "reg_slots" (register slots R = 3, 4, 5 per tile-pass thread: 2^R amplitudes
  * each; raised to the widest fused block), "max_stages", "budget", "nbuf",
- * "ctas_per_sm", "eager", "fuse", "flush_ops", "profile".  0 = ok, -1 =
- * unknown key or bad value. */
+ * "ctas_per_sm", "eager", "fuse", "flush_ops", "profile", "jit" (tile passes
+ * run by kernels generated for each pass's structure and compiled with NVRTC:
+ * 0 off; 1, the default, compiles a recorded program's kernels at record_end
+ * and lets flushes use kernels already compiled for their structure, queuing
+ * the missing ones for compilation on background threads, for arrays of at
+ * least 2^18 amplitudes; 2 compiles before every first launch, any size).
+ * 0 = ok, -1 = unknown key or bad value. */
 int iq_handle_set_option(void* h, const char* key, double value);
 double iq_handle_get_option(void* h, const char* key);
 /* Counters: out[0] passes, [1] operations applied, [2] algorithmic bytes moved by
  * passes, [3] kernel launches, [4] flushes, [5] tile-pass launches, [6] bytes of
- * operation matrices copied host->device by flushes.  Returns the number of
- * values written. */
+ * operation matrices copied host->device by flushes, [7] tile passes run by a
+ * specialised kernel.  Returns the number of values written. */
 int iq_handle_stats(void* h, double* out, size_t n);
+/* Specialised pass kernels of the process: out[0] compiled with NVRTC, [1]
+ * loaded from the cubin cache directory (IQ_JIT_CACHE, default
+ * ~/.cache/invariantq_b200/jit, "off" = none); `note` gets why the last
+ * compilation attempt failed ("" if none).  Returns the values written. */
+int iq_jit_info(double* out, size_t n, char* note, size_t note_len);
+/* Wait up to timeout_s for background compilations to finish: 0 = idle. */
+int iq_jit_wait(double timeout_s);
 /* Recorded programs: operations issued between record_begin and record_end are
  * planned once into tile passes whose matrices and descriptors stay on the
  * device; program_run launches them on the handle's stream (any number of

@@ -116,6 +116,8 @@ SIGNATURES = {
     "iq_ansatz_energy": ([ctypes.POINTER(AdjointCircuit)], _i),
     "iq_adjoint_stats": ([c_dp, _sz], _i),
     "iq_selftest_bounded_wait": ([_d, c_dp], _i),
+    "iq_jit_info": ([c_dp, _sz, ctypes.c_char_p, _sz], _i),
+    "iq_jit_wait": ([_d], _i),
     "iq_adjoint_release": ([], _i),
     "iq_density_matrix_flush": ([_v], _i),
     "iq_density_matrix_apply_kraus_2q": ([_v, _sz, _sz, _sz, c_dp, c_dp], None),

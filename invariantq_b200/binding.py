@@ -45,9 +45,9 @@ class _Handle:
         return self._lib.iq_handle_get_option(self._ptr, key.encode())
 
     def stats(self) -> Dict[str, float]:
-        out = np.zeros(7)
-        self._lib.iq_handle_stats(self._ptr, _p(out), 7)
-        keys = ("passes", "ops", "bytes", "launches", "flushes", "tile_passes", "h2d_bytes")
+        out = np.zeros(8)
+        self._lib.iq_handle_stats(self._ptr, _p(out), 8)
+        keys = ("passes", "ops", "bytes", "launches", "flushes", "tile_passes", "h2d_bytes", "jit_passes")
         return dict(zip(keys, out.tolist()))
 
     def record(self):
@@ -352,3 +352,17 @@ def selftest_bounded_wait(limit_ms: float = 20.0) -> tuple:
         check(lib)
         raise RuntimeError("iq_selftest_bounded_wait failed")
     return st, waited.value
+
+
+def jit_info() -> dict:
+    """Specialised pass kernels of this process (iq_jit_info)."""
+    lib = _lib.load()
+    out = np.zeros(2)
+    note = ctypes.create_string_buffer(512)
+    lib.iq_jit_info(_p(out), 2, note, 512)
+    return {"compiled": int(out[0]), "from_disk": int(out[1]), "note": note.value.decode(errors="replace")}
+
+
+def jit_wait(timeout_s: float = 120.0) -> bool:
+    """Wait for background kernel compilations (iq_jit_wait); True when idle."""
+    return _lib.load().iq_jit_wait(float(timeout_s)) == 0

@@ -27,8 +27,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", *ARCH]
 SOURCES = ["iq_tile_r3.cu", "iq_tile_r4.cu", "iq_tile_r5.cu", "iq_kernels.cu", "iq_runtime.cu", "iq_sched.cpp", "iq_noalloc.cu",
            "iq_adjoint.cu", "iq_c64.cu",
-           "iq_selftest.cu"]
-HEADERS = ["iq_kernels.h", "iq_plan.h", "iq_tile.cuh", "iq_c64.h"]
+           "iq_selftest.cu", "iq_jit.cpp", "iq_jitgen.cpp"]
+HEADERS = ["iq_kernels.h", "iq_plan.h", "iq_pipe.cuh", "iq_tile.cuh", "iq_c64.h", "iq_jit.h"]
+# headers the run-time compiled pass kernels include, embedded into the library
+JIT_HEADERS = ["iq_plan.h", "iq_pipe.cuh"]
+JIT_INC = CSRC / "iq_jit_headers.inc"
 
 
 def nvcc() -> str:
@@ -39,7 +42,7 @@ def nvcc() -> str:
 
 
 def _newest_dep() -> float:
-    deps = [CSRC / h for h in HEADERS] + [INCLUDE / "invariantq_b200.h", Path(__file__)]
+    deps = [CSRC / h for h in HEADERS] + [JIT_INC, INCLUDE / "invariantq_b200.h", Path(__file__)]
     return max(p.stat().st_mtime for p in deps if p.exists())
 
 
@@ -57,8 +60,26 @@ def _compile(src: str, force: bool, dep_time: float) -> tuple[str, str]:
     return src, r.stderr
 
 
+def _write_jit_headers() -> None:
+    """iq_jit_headers.inc: the JIT headers as raw string literals (rewritten
+    only when their text changes, so unchanged builds stay incremental)."""
+    names, texts = [], []
+    for h in JIT_HEADERS:
+        t = (CSRC / h).read_text()
+        if ")IQJIT\"" in t:
+            raise RuntimeError(f"{h} contains the raw-string delimiter")
+        names.append(f'"{h}"')
+        texts.append(f'R"IQJIT({t})IQJIT"')
+    body = ("// generated by invariantq_b200/build.py from " + ", ".join(JIT_HEADERS) + "\n"
+            "static const char* const kJitHeaderNames[] = {" + ", ".join(names) + "};\n"
+            "static const char* const kJitHeaderSources[] = {\n" + ",\n".join(texts) + "};\n")
+    if not JIT_INC.exists() or JIT_INC.read_text() != body:
+        JIT_INC.write_text(body)
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
+    _write_jit_headers()
     dep_time = _newest_dep()
     with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         results = list(ex.map(lambda s: _compile(s, force, dep_time), SOURCES))

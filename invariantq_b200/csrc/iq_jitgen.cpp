@@ -1,0 +1,204 @@
+// iq_jitgen.cpp -- source generator of the per-pass tile kernels (compiled
+// at run time by iq_jit.cpp).  Pure C++: the CPU tests link it with the
+// scheduler and compile its output with NVRTC.
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "iq_plan.h"
+
+namespace iqb {
+
+namespace {
+
+struct Gen {
+  std::ostringstream o;
+  int tmp = 0;
+  std::string fresh() { return "t" + std::to_string(tmp++); }
+};
+
+std::string mat(uint32_t i) { return "Mt.m[" + std::to_string(i) + "]"; }
+
+// Straight-line code of one stage.  cur[v] names the value register v of the
+// thread holds (v's bit i = register slot i).  Every operation is written with
+// the interpreting kernel's expression for it (iq_tile.cuh), so the results
+// agree bit for bit.
+bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
+  const StageDesc& sd = d.st[s];
+  const int R = d.R, NV = 1 << R;
+  std::ostringstream& o = g.o;
+  uint32_t sb[kMaxK];
+  for (int i = 0; i < R; ++i) sb[i] = swz(1u << sd.S[i]);
+  auto voffc = [&](int v) {
+    uint32_t x = 0;
+    for (int i = 0; i < R; ++i)
+      if ((v >> i) & 1) x ^= sb[i];
+    return x;
+  };
+  o << "    {  // stage " << s << "\n";
+  o << "      const unsigned lo = ((unsigned)(lane8 & 1) << " << (int)sd.lane[0] << ") | ((unsigned)((lane8 >> 1) & 1) << "
+    << (int)sd.lane[1] << ") | ((unsigned)((lane8 >> 2) & 1) << " << (int)sd.lane[2] << ");\n";
+  o << "      for (int u = octet; u < " << (1 << sd.nt) << "; u += " << NT / 8 << ") {\n";
+  o << "        unsigned base = lo";
+  for (int i = 0; i < sd.nt; ++i) o << " | ((((unsigned)u >> " << i << ") & 1u) << " << (int)sd.tb[i] << ")";
+  o << ";\n        base = swz(base);\n";
+  std::vector<std::string> cur(NV);
+  for (int v = 0; v < NV; ++v) {
+    cur[v] = g.fresh();
+    o << "        const double2 " << cur[v] << " = tile[base ^ " << voffc(v) << "u];\n";
+  }
+  auto def = [&](const std::string& expr) {
+    const std::string n = g.fresh();
+    o << "        const double2 " << n << " = " << expr << ";\n";
+    return n;
+  };
+  for (int oi = sd.op0; oi < sd.op1; ++oi) {
+    const OpDesc& od = d.ops[oi];
+    const uint32_t m = od.mat;
+    const bool unit = od.flags & OPF_UNIT_PHASE;
+    switch (od.kind) {
+      case OP_D1R: {
+        const int A = 1 << od.a;
+        for (int v = 0; v < NV; ++v) {
+          if (v & A) continue;
+          const std::string x = cur[v], y = cur[v | A];
+          cur[v] = def("cfma(cmul(" + mat(m + 0) + ", " + x + "), " + mat(m + 1) + ", " + y + ")");
+          cur[v | A] = def("cfma(cmul(" + mat(m + 2) + ", " + x + "), " + mat(m + 3) + ", " + y + ")");
+        }
+        break;
+      }
+      case OP_M1R: {
+        const int A = 1 << od.a;
+        const bool sw = od.perm & 1;
+        for (int v = 0; v < NV; ++v) {
+          if (v & A) continue;
+          std::string x = cur[v], y = cur[v | A];
+          if (sw) std::swap(x, y);
+          if (!unit) {
+            x = def("cmul(" + mat(m + 0) + ", " + x + ")");
+            y = def("cmul(" + mat(m + 1) + ", " + y + ")");
+          }
+          cur[v] = x;
+          cur[v | A] = y;
+        }
+        break;
+      }
+      case OP_D1L: {
+        const int l = od.a;
+        const std::string hi = g.fresh(), cs = g.fresh(), co = g.fresh();
+        o << "        const bool " << hi << " = (lane8 >> " << l << ") & 1;\n";
+        o << "        const double2 " << cs << " = " << hi << " ? " << mat(m + 3) << " : " << mat(m + 0) << ";\n";
+        o << "        const double2 " << co << " = " << hi << " ? " << mat(m + 2) << " : " << mat(m + 1) << ";\n";
+        for (int v = 0; v < NV; ++v) {
+          const std::string p = def("shfl_xor2(" + cur[v] + ", " + std::to_string(1 << l) + ", omask)");
+          cur[v] = def("cfma(cmul(" + cs + ", " + cur[v] + "), " + co + ", " + p + ")");
+        }
+        break;
+      }
+      case OP_M1L: {
+        const int l = od.a;
+        const bool sw = od.perm & 1;
+        std::string ph;
+        if (!unit) {
+          const std::string hi = g.fresh();
+          ph = g.fresh();
+          o << "        const bool " << hi << " = (lane8 >> " << l << ") & 1;\n";
+          o << "        const double2 " << ph << " = " << hi << " ? " << mat(m + 1) << " : " << mat(m + 0) << ";\n";
+        }
+        for (int v = 0; v < NV; ++v) {
+          std::string x = cur[v];
+          if (sw) x = def("shfl_xor2(" + x + ", " + std::to_string(1 << l) + ", omask)");
+          if (!unit) x = def("cmul(" + ph + ", " + x + ")");
+          cur[v] = x;
+        }
+        break;
+      }
+      case OP_D2R: {
+        const int A = 1 << od.a, B = 1 << od.b;
+        for (int v = 0; v < NV; ++v) {
+          if (v & (A | B)) continue;
+          const int idx[4] = {v, v | A, v | B, v | A | B};
+          const std::string x[4] = {cur[idx[0]], cur[idx[1]], cur[idx[2]], cur[idx[3]]};
+          for (int r = 0; r < 4; ++r) {
+            std::string e = "cmul(" + mat(m + 4 * r) + ", " + x[0] + ")";
+            for (int c = 1; c < 4; ++c) e = "cfma(" + e + ", " + mat(m + 4 * r + c) + ", " + x[c] + ")";
+            cur[idx[r]] = def(e);
+          }
+        }
+        break;
+      }
+      case OP_M2R: {
+        const int A = 1 << od.a, B = 1 << od.b;
+        for (int v = 0; v < NV; ++v) {
+          if (v & (A | B)) continue;
+          const int idx[4] = {v, v | A, v | B, v | A | B};
+          const std::string x[4] = {cur[idx[0]], cur[idx[1]], cur[idx[2]], cur[idx[3]]};
+          for (int r = 0; r < 4; ++r) {
+            const std::string y = x[(od.perm >> (2 * r)) & 3];
+            cur[idx[r]] = unit ? y : def("cmul(" + mat(m + r) + ", " + y + ")");
+          }
+        }
+        break;
+      }
+      case OP_DKR: {
+        const int D = 1 << od.k;
+        if (od.k > R) { err = "dense block wider than the register slots"; return false; }
+        std::vector<std::string> out(NV);
+        for (int gb = 0; gb < NV; gb += D)
+          for (int r = 0; r < D; ++r) {
+            std::string e = "cmul(" + mat(m + r * D) + ", " + cur[gb] + ")";
+            for (int c = 1; c < D; ++c) e = "cfma(" + e + ", " + mat(m + r * D + c) + ", " + cur[gb + c] + ")";
+            out[gb + r] = def(e);
+          }
+        cur = out;
+        break;
+      }
+      default:
+        err = "operation kind " + std::to_string((int)od.kind) + " is not specialised";
+        return false;
+    }
+  }
+  for (int v = 0; v < NV; ++v) o << "        tile[base ^ " << voffc(v) << "u] = " << cur[v] << ";\n";
+  o << "      }\n    }\n    __syncthreads();\n";
+  return true;
+}
+
+}  // namespace
+
+// Source of the kernel specialised to pass `d` (see iq_plan.h).
+std::string jit_pass_source(const PassDesc& d, std::string& err) {
+  if (d.ngrad || d.nsets > 1) {
+    err = "adjoint passes are not specialised";
+    return "";
+  }
+  if (d.R < 3 || d.R > kMaxK) {
+    err = "register slots out of range";
+    return "";
+  }
+  const int NT = tile_pass_threads(d.R);
+  const int MINB = d.R == 5 ? 1 : 2;
+  const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
+  Gen g;
+  std::ostringstream& o = g.o;
+  o << "// generated by iq_jitgen (iq-jit-1): M=" << (int)d.M << " c=" << (int)d.c << " R=" << (int)d.R
+    << " stages=" << (int)d.nstages << " ops=" << d.nops << "\n";
+  o << "#include \"iq_pipe.cuh\"\nusing namespace iqb;\n";
+  o << "struct JitMats { double2 m[" << nmat << "]; };\n";
+  o << "struct JitBody {\n  const JitMats& Mt;\n  int lane8, octet;\n  unsigned omask;\n";
+  o << "  __device__ __forceinline__ void operator()(double2* tile, unsigned long long, bool work) {\n";
+  o << "    if (!work) return;\n";
+  for (int s = 0; s < d.nstages; ++s)
+    if (!gen_stage(g, d, s, NT, err)) return "";
+  o << "  }\n};\n";
+  o << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << MINB << ")\n"
+    << "iq_jit_pass(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,\n"
+    << "            const __grid_constant__ JitMats Mt, int* __restrict__ status, int nbuf) {\n"
+    << "  extern __shared__ __align__(1024) unsigned char smem_raw[];\n"
+    << "  double2* tiles = aligned_tiles(smem_raw);\n"
+    << "  const int ctid = threadIdx.x;\n"
+    << "  JitBody body{Mt, ctid & 7, ctid >> 3, 0xFFu << (ctid & 24)};\n"
+    << "  tile_pipeline<" << NT << ">(tm, P, tiles, status, nbuf, body);\n}\n";
+  return o.str();
+}
+
+}  // namespace iqb

@@ -8,13 +8,6 @@
 
 namespace iqb {
 
-// Error codes a kernel can raise in the per-handle device status word.
-enum DevErr : int {
-  DEV_OK = 0,
-  DEV_WAIT_LOADED = 1,     // a tile load did not complete in the wait limit
-  DEV_WAIT_COMPUTED = 2,   // the producer waited too long for the consumers
-};
-
 struct TileLaunch {
   int nbuf;                // shared-memory tile buffers per CTA (pipeline depth)
   int ctas_per_sm;         // resident CTAs per SM the grid is sized for
@@ -28,10 +21,6 @@ int encode_pass_tmap(CUtensorMap* tm, void* state, int nbits, const PassDesc& d,
 // grad_partials: [gradient term][CTA] partial sums of the pass's OP_GRAD2 terms (or null)
 cudaError_t launch_tile_pass(const CUtensorMap& tm, const PassDesc& d, const double2* mats, int* dev_status,
                              const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials = nullptr);
-// Threads per tile-pass CTA for R register slots: R = 3 (8 amplitudes per
-// thread, <= 128 registers) runs 256 threads so a 2^11 tile is still one row
-// set per stage and twice the warps are resident; R = 4, 5 run 128.
-constexpr int tile_pass_threads(int R) { return R == 3 ? 256 : 128; }
 // dynamic shared memory of a pass: tile buffers, matrix block, gradient accumulators
 size_t tile_pass_smem_bytes(int M, int R, int nbuf, uint32_t mat_elems, uint32_t ngrad);
 // one launcher per kernel instantiation (iq_tile_r3.cu, iq_tile_r4.cu, iq_tile_r5.cu)

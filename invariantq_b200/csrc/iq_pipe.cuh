@@ -1,0 +1,279 @@
+// iq_pipe.cuh -- device code shared by the tile-pass kernels: complex
+// arithmetic helpers, mbarrier / TMA wrappers, bounded waits, and the tile
+// pipeline (a ring of shared-memory tile buffers fed and drained by TMA tensor
+// copies).  The interpreting kernel (iq_tile.cuh) and the kernels generated
+// per pass at run time (iq_jit.cpp, compiled with NVRTC) both run their
+// stages inside tile_pipeline(), so both move tiles the same way.  The file
+// compiles under nvcc and under NVRTC (__CUDACC_RTC__: no system headers).
+#pragma once
+#if defined(__CUDACC_RTC__)
+struct __align__(64) CUtensorMap { unsigned long long opaque[16]; };   // layout of the driver's 128-byte map
+#else
+#include <cuda.h>
+#include <cuda_runtime.h>
+#endif
+
+#include "iq_plan.h"
+
+namespace iqb {
+
+// ------------------------------------------------------------------ helpers
+
+// explicit FMA forms: the interpreting and the generated kernels contract
+// every complex product the same way, whatever the operands' origin
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cfma(double2 acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+// operation matrices are read from the pass's block in shared memory
+__device__ __forceinline__ double2 ld_mat(const double2* m, int i) { return m[i]; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done;
+}
+
+// try_wait that lets the hardware park the thread until the phase completes or
+// `hint_ns` passes, so a waiting warp issues no instructions meanwhile (a plain
+// try_wait returns almost at once and the polling loop would take issue slots
+// from the warps that compute)
+constexpr uint32_t kWaitSuspendNs = 20000;
+__device__ __forceinline__ uint32_t mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return done;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
+                                             const void* src) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
+      " [%0, {%2, %3, %4, %5, %6}], [%1];" ::"l"(tm),
+      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Wait limit of one mbarrier phase: 2 s of %globaltimer (a tile load or a
+// consumer stage takes microseconds).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait that ignores the abort flag: used to let copies already in
+// flight land before the CTA exits after an abort.
+__device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait_suspend(bar, parity, kWaitSuspendNs))
+    if (global_ns() - t0 > kWaitLimitNs) return;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false (and raises the abort flag
+// plus the status word) when the limit runs out, or as soon as another thread
+// of the CTA has aborted.
+__device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                             int* status, int code, uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait_suspend(bar, parity, kWaitSuspendNs)) return true;
+    if (*abort_flag) return false;
+    if (global_ns() - t0 > limit_ns) break;
+  }
+  *abort_flag = 1;
+  atomicCAS(status, 0, code);
+  return false;
+}
+
+
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
+  return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
+}
+
+constexpr int kMaxBuf = 4;
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// The tile pipeline of one pass (NT threads, all of them compute; the lanes
+// of every warp also issue the TMA copies).  Tiles cycle through `nbuf`
+// shared-memory buffers at `tiles` (1024-byte aligned for the 128-byte
+// swizzle): while tile i is computed, tiles up to i + depth are loading and
+// the stores of earlier tiles are draining.  depth = nbuf - 2 for nbuf >= 3,
+// else nbuf - 1, so the buffer a load re-arms always held a tile every thread
+// has finished with, and its mbarrier is armed once per phase.
+//
+// body(buf, t, work) runs the pass's stages on the resident tile buf (global
+// tile index t) with a __syncthreads() after each stage; `work` is uniform in
+// the CTA and false after an abort (the body must then only keep the CTA's
+// barriers in step).  Every thread of the CTA calls tile_pipeline.
+template <int NT, class Body>
+__device__ __forceinline__ void tile_pipeline(const CUtensorMap& tm, const PassDesc& P, double2* tiles,
+                                              int* __restrict__ status, int nbuf, Body&& body) {
+  __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
+  __shared__ volatile int abort_flag;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const uint32_t tile_elems = 1u << P.M;
+  const uint64_t ntiles = P.ntiles;
+  const uint64_t first = blockIdx.x;
+  if (tid == 0) {
+    for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
+    abort_flag = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  const uint64_t cnt = (first < ntiles) ? (ntiles - 1 - first) / gridDim.x + 1 : 0;
+  const int depth = nbuf >= 3 ? nbuf - 2 : nbuf - 1;   // < nbuf
+
+  // ---- copy issue setup: every warp issues its share of a tile's copies
+  // (issues j = warp + NW * (lane + 32 r)); the tile mbarrier expects one
+  // arrival per warp.  Coordinates are linear in the disjoint address bits, so
+  // each lane keeps the offsets of its issues and adds the tile's base
+  // coordinates per tile.
+  constexpr int NW = NT / 32;
+  const int warp = tid >> 5;
+  const int nbox = P.nbox;
+  const int nissue = 1 << (P.nH - nbox);
+  const uint32_t box_elems = 1u << (P.c + nbox);
+  const uint32_t box_bytes = box_elems * 16u;
+  constexpr int kMaxPerLane = 1;   // nissue <= 32 * NW
+  int jc1[kMaxPerLane], jc3[kMaxPerLane], jc4[kMaxPerLane], jj[kMaxPerLane];
+  uint32_t my_bytes = 0;           // bytes of this warp's issues per tile
+#pragma unroll
+  for (int r = 0; r < kMaxPerLane; ++r) {
+    const int j = warp + NW * (lane + 32 * r);
+    jj[r] = j;
+    int c2;
+    if (j < nissue) chunk_coords(issue_offset(j, P), P, jc1[r], c2, jc3[r], jc4[r]);
+    else jc1[r] = jc3[r] = jc4[r] = 0;
+  }
+  for (int j = warp; j < nissue; j += NW) my_bytes += box_bytes;
+  TileCoordMap cmap;               // tile index -> tensor-map coordinates (32-bit, per thread)
+  tile_coord_map(P, cmap);
+  auto base_coords = [&](uint64_t t, int& c1, int& c3, int& c4) {
+    int c2;
+    tile_coords((uint32_t)t, cmap, c1, c2, c3, c4);
+  };
+  auto issue_load = [&](uint64_t i) {   // whole warp, converged
+    const int b = (int)(i % nbuf);
+    int c1, c3, c4;
+    base_coords(first + i * gridDim.x, c1, c3, c4);
+    double2* buf = tiles + (size_t)b * tile_elems;
+    if (lane == 0) mbar_arrive_expect_tx(&bar_loaded[b], my_bytes);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kMaxPerLane; ++r)
+      if (jj[r] < nissue)
+        tma_load_5d(buf + (size_t)jj[r] * box_elems, &tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r],
+                    &bar_loaded[b]);
+  };
+  auto issue_store = [&](uint64_t i) {  // whole warp; one bulk group per lane per tile
+    const int b = (int)(i % nbuf);
+    int c1, c3, c4;
+    base_coords(first + i * gridDim.x, c1, c3, c4);
+    double2* buf = tiles + (size_t)b * tile_elems;
+#pragma unroll
+    for (int r = 0; r < kMaxPerLane; ++r)
+      if (jj[r] < nissue)
+        tma_store_5d(&tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r], buf + (size_t)jj[r] * box_elems);
+    bulk_commit();
+  };
+
+  uint64_t issued = 0;             // tiles whose loads have been issued
+  uint64_t first_unwaited = cnt;   // first tile whose load wait did not succeed
+  for (; issued < (uint64_t)depth && issued < cnt; ++issued) issue_load(issued);
+
+  for (uint64_t i = 0; i < cnt; ++i) {
+    const int b = (int)(i % nbuf);
+    // abort_flag is read after the previous iteration's barrier: uniform in the CTA
+    const bool ab = __shfl_sync(0xffffffffu, (int)abort_flag, 0) != 0;
+    if (i + depth < cnt && !ab) {
+      // buffer (i + depth) % nbuf last held tile i + depth - nbuf (finished by
+      // every thread: it is at most tile i - 1), whose store is followed by
+      // nbuf - depth - 1 later stores: wait only for that store's read
+      if (i + depth >= (uint64_t)nbuf) {
+        if (nbuf - depth - 1 >= 1) bulk_wait_read<1>();
+        else bulk_wait_read<0>();
+      }
+      __syncwarp();
+      issue_load(i + depth);
+      issued = i + depth + 1;
+    }
+    const bool ok = bounded_wait(&bar_loaded[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status, DEV_WAIT_LOADED);
+    const bool work = __syncthreads_and(ok && !abort_flag);
+    if (!work && first_unwaited == cnt) first_unwaited = i;
+    double2* buf = tiles + (size_t)b * tile_elems;
+    body(buf, first + i * gridDim.x, work);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (work) issue_store(i);
+  }
+  // after an abort, let loads that were issued but never consumed land first
+  for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
+  bulk_wait_all();
+}
+
+// 1024-byte aligned start of the dynamic shared memory (the tile buffers)
+__device__ __forceinline__ double2* aligned_tiles(unsigned char* smem_raw) {
+  return reinterpret_cast<double2*>((reinterpret_cast<unsigned long long>(smem_raw) + 1023ull) & ~1023ull);
+}
+
+}  // namespace iqb

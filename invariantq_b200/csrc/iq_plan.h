@@ -18,8 +18,16 @@
 // The C ABI's 2-qubit calls (q0 = most significant) are converted to this form
 // before they reach the scheduler.
 #pragma once
+#if defined(__CUDACC_RTC__)
+// runtime-compiled kernels (NVRTC): no system headers
+typedef unsigned char uint8_t;
+typedef unsigned short uint16_t;
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+#else
 #include <stdint.h>
 #include <stddef.h>
+#endif
 
 #if defined(__CUDACC__)
 #define IQ_HD __host__ __device__ __forceinline__
@@ -36,6 +44,18 @@ constexpr int kMaxPassOps = 160;
 constexpr int kMaxK = 5;           // widest dense block the kernels apply
 constexpr int kSmemMatElems = 1024; // per-pass matrix block kept in shared memory (16 KiB)
 constexpr int kMaxPassGrads = 64;   // gradient terms accumulated by one pass
+
+// Error codes a kernel can raise in the per-handle device status word.
+enum DevErr : int {
+  DEV_OK = 0,
+  DEV_WAIT_LOADED = 1,     // a tile load did not complete in the wait limit
+  DEV_WAIT_COMPUTED = 2,   // the producer waited too long for the consumers
+};
+
+// Threads per tile-pass CTA for R register slots: R = 3 (8 amplitudes per
+// thread, <= 128 registers) runs 256 threads so a 2^11 tile is still one row
+// set per stage and twice the warps are resident; R = 4, 5 run 128.
+constexpr int tile_pass_threads(int R) { return R == 3 ? 256 : 128; }
 
 enum OpKind : uint8_t {
   OP_NONE = 0,
@@ -269,12 +289,17 @@ IQ_HD void tile_coords(uint32_t t, const TileCoordMap& m, int& c1, int& c2, int&
 
 }  // namespace iqb
 
-#ifdef __cplusplus
+#if defined(__cplusplus) && !defined(__CUDACC_RTC__)
 #include <string>
 #include <vector>
 namespace iqb {
 int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vector<PassPlan>& out,
                 std::string& err);
+// Source of the tile kernel specialised to pass `d` (iq_jitgen.cpp): stage
+// layout, operations and matrix offsets fixed; tile bits, tile count and
+// matrix values stay launch parameters.  Returns "" and sets `err` for a pass
+// that is not specialised (adjoint steps, several parameter sets).
+std::string jit_pass_source(const PassDesc& d, std::string& err);
 struct cplx64 { double re, im; };
 // Fuse runs of queued operations on at most two qubits into single 4x4 blocks
 // (a two-qubit operation absorbs the open one-qubit blocks of its qubits and

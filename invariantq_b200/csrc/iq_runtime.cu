@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/invariantq_b200.h"
+#include "iq_jit.h"
 #include "iq_kernels.h"
 #include "iq_plan.h"
 
@@ -159,6 +160,15 @@ double entropy_from(const std::vector<double>& eig) {
   return s > 0.0 ? s : 0.0;
 }
 
+// why the last attempt to compile specialised pass kernels failed (the
+// interpreting kernel ran those passes)
+std::mutex g_jit_mu;
+std::string g_jit_note;
+void jit_note(const std::string& why) {
+  std::lock_guard<std::mutex> lk(g_jit_mu);
+  g_jit_note = why;
+}
+
 // ---------------------------------------------------------------- engine
 
 constexpr size_t kStageBytes = 64ull << 20;   // device/host staging for readbacks
@@ -196,9 +206,16 @@ struct Engine {
   int fuse = 1;
   int flush_ops = 4096;
   int profile = 0;
+  // Specialised pass kernels (iq_jit.cpp): 0 off; 1 recorded programs are
+  // compiled when recorded and flushes use kernels already compiled for their
+  // structure (missing ones compile in the background), for arrays of at least
+  // 2^kJitMinBits amplitudes; 2 both compiled before their first launch, any size.
+  int jit = 1;
+  static constexpr int kJitMinBits = 18;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
 
   double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0, st_h2d = 0;
+  double st_jit = 0;                 // tile passes run by a specialised kernel
   bool recording = false;
 
   bool init(int kind_, size_t n) {
@@ -375,7 +392,30 @@ struct Engine {
     bool owns = false;
     size_t pool_elems = 0;
     int nops = 0;
+    std::vector<const JitKernel*> jit;   // specialised kernel per pass (null: interpreting kernel)
+    std::vector<cplx64> hmats;           // host copy of the pass matrix blocks (launch parameters)
   };
+
+  // kernels specialised to the program's passes: compiled now (recorded
+  // programs, jit 2) or taken from those already compiled (flushes)
+  void attach_jit(Program& pg, bool own, std::vector<cplx64>& packed) {
+    if (!jit || (jit == 1 && nbits < kJitMinBits) || pg.plans.empty()) return;
+    std::vector<const PassDesc*> ds;
+    for (auto& pl : pg.plans) ds.push_back(&pl.desc);
+    if (own || jit >= 2) {
+      std::string err;
+      if (!jit_prepare(ds, pg.jit, err)) {
+        jit_note(err);
+        pg.jit.clear();
+      }
+    } else {
+      jit_lookup(ds, pg.jit, true);
+    }
+    bool any = false;
+    for (auto* k : pg.jit) any |= k != nullptr;
+    if (any) pg.hmats = std::move(packed);
+    else pg.jit.clear();
+  }
 
   bool build_program(Program& pg, bool own) {
     pg.nops = (int)ops.size();
@@ -427,6 +467,7 @@ struct Engine {
       if (!upload_pool(reinterpret_cast<const double2*>(src), nsrc)) return false;
       pg.d_mats = d_pool;
     }
+    if (pg.tiled) attach_jit(pg, own, packed);
     return true;
   }
 
@@ -449,9 +490,18 @@ struct Engine {
         cudaEventCreate(&e1);
         cudaEventRecord(e0, stream);
       }
-      if (!cuda_ok(launch_tile_pass(pg.tmaps[i], pg.plans[i].desc, pg.d_mats, d_status, tl, num_sms, stream),
-                   "tile pass kernel"))
+      const PassDesc& desc = pg.plans[i].desc;
+      if (i < pg.jit.size() && pg.jit[i]) {
+        if (!cuda_ok(jit_launch(pg.jit[i], pg.tmaps[i], desc,
+                                reinterpret_cast<const double2*>(pg.hmats.data()) + desc.mat_base, d_status, tl,
+                                num_sms, stream),
+                     "specialised tile pass kernel"))
+          return false;
+        ++st_jit;
+      } else if (!cuda_ok(launch_tile_pass(pg.tmaps[i], desc, pg.d_mats, d_status, tl, num_sms, stream),
+                          "tile pass kernel")) {
         return false;
+      }
       if (profile) {
         cudaEventRecord(e1, stream);
         prof.emplace_back(e0, e1);
@@ -1066,6 +1116,7 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "fuse")) e->fuse = iv ? 1 : 0;
   else if (!strcmp(key, "flush_ops")) { if (iv < 1) return -1; e->flush_ops = iv; }
   else if (!strcmp(key, "profile")) e->profile = iv ? 1 : 0;
+  else if (!strcmp(key, "jit")) { if (iv < 0 || iv > 2) return -1; e->jit = iv; }
   else if (!strcmp(key, "inject_status")) {   // failure-path tests: as if a tile pass had timed out
     if (iv < 1 || iv > 2) return -1;
     if (!cuda_ok(cudaMemcpyAsync(e->d_status, &iv, sizeof(int), cudaMemcpyHostToDevice, e->stream), "inject status") ||
@@ -1091,14 +1142,16 @@ double iq_handle_get_option(void* h, const char* key) {
   if (!strcmp(key, "fuse")) return e->fuse;
   if (!strcmp(key, "flush_ops")) return e->flush_ops;
   if (!strcmp(key, "profile")) return e->profile;
+  if (!strcmp(key, "jit")) return e->jit;
   return kNaN;
 }
 
 int iq_handle_stats(void* h, double* out, size_t n) {
   Engine* e = static_cast<Engine*>(h);
   if (!e || !out) return 0;
-  const double v[7] = {e->st_passes, e->st_ops, e->st_bytes, e->st_launches, e->st_flushes, e->st_tile, e->st_h2d};
-  const size_t m = std::min<size_t>(n, 7);
+  const double v[8] = {e->st_passes, e->st_ops, e->st_bytes,  e->st_launches,
+                       e->st_flushes, e->st_tile, e->st_h2d, e->st_jit};
+  const size_t m = std::min<size_t>(n, 8);
   for (size_t i = 0; i < m; ++i) out[i] = v[i];
   return (int)m;
 }
@@ -1176,6 +1229,23 @@ void iq_program_free(void* prog) {
   if (pg->owns && pg->d_mats) cudaFree(pg->d_mats);
   delete pg;
 }
+
+// ============================================================ specialised kernels
+
+int iq_jit_info(double* out, size_t n, char* note, size_t note_len) {
+  uint64_t compiled = 0, disk = 0;
+  jit_counters(&compiled, &disk);
+  const double v[2] = {(double)compiled, (double)disk};
+  const size_t m = out ? std::min<size_t>(n, 2) : 0;
+  for (size_t i = 0; i < m; ++i) out[i] = v[i];
+  if (note && note_len) {
+    std::lock_guard<std::mutex> lk(g_jit_mu);
+    snprintf(note, note_len, "%s", g_jit_note.c_str());
+  }
+  return (int)m;
+}
+
+int iq_jit_wait(double timeout_s) { return jit_wait(timeout_s > 0 ? timeout_s : 0.0) ? 0 : -1; }
 
 // ============================================================ density matrix
 

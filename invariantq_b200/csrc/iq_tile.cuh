@@ -21,6 +21,7 @@
 #include <atomic>
 
 #include "iq_kernels.h"
+#include "iq_pipe.cuh"
 
 namespace iqb {
 
@@ -45,126 +46,6 @@ inline cudaError_t allow_full_dynamic_smem(K kern, std::atomic<uint64_t>& done) 
   r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
   if (r == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
   return r;
-}
-
-// ------------------------------------------------------------------ helpers
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cfma(double2 acc, double2 a, double2 b) {
-  acc.x = fma(a.x, b.x, acc.x);
-  acc.x = fma(-a.y, b.y, acc.x);
-  acc.y = fma(a.x, b.y, acc.y);
-  acc.y = fma(a.y, b.x, acc.y);
-  return acc;
-}
-// operation matrices are read from the pass's block in shared memory
-__device__ __forceinline__ double2 ld_mat(const double2* m, int i) { return m[i]; }
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return done;
-}
-
-// try_wait that lets the hardware park the thread until the phase completes or
-// `hint_ns` passes, so a waiting warp issues no instructions meanwhile (a plain
-// try_wait returns almost at once and the polling loop would take issue slots
-// from the warps that compute)
-constexpr uint32_t kWaitSuspendNs = 20000;
-__device__ __forceinline__ uint32_t mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
-      : "memory");
-  return done;
-}
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
-                                            int c4, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
-      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void tma_store_5d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
-                                             const void* src) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group"
-      " [%0, {%2, %3, %4, %5, %6}], [%1];" ::"l"(tm),
-      "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
-      : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-// Wait limit of one mbarrier phase: 2 s of %globaltimer (a tile load or a
-// consumer stage takes microseconds).
-constexpr uint64_t kWaitLimitNs = 2000000000ull;
-
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait that ignores the abort flag: used to let copies already in
-// flight land before the CTA exits after an abort.
-__device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity) {
-  const uint64_t t0 = global_ns();
-  while (!mbar_try_wait_suspend(bar, parity, kWaitSuspendNs))
-    if (global_ns() - t0 > kWaitLimitNs) return;
-}
-
-// Bounded wait on an mbarrier phase.  Returns false (and raises the abort flag
-// plus the status word) when the limit runs out, or as soon as another thread
-// of the CTA has aborted.
-__device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                             int* status, int code, uint64_t limit_ns = kWaitLimitNs) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_ns();
-  for (;;) {
-    if (mbar_try_wait_suspend(bar, parity, kWaitSuspendNs)) return true;
-    if (*abort_flag) return false;
-    if (global_ns() - t0 > limit_ns) break;
-  }
-  *abort_flag = 1;
-  atomicCAS(status, 0, code);
-  return false;
 }
 
 // ------------------------------------------------------- register-slot ops
@@ -371,9 +252,6 @@ __device__ __forceinline__ void dkr_store(const double2 (&a)[1 << R], const doub
 }
 
 // lane-bit 1q ops: partner amplitude lives in lane ^ (1 << lb) of the octet
-__device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
-  return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
-}
 
 template <int R>
 __device__ __forceinline__ void d1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
@@ -646,141 +524,31 @@ __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int 
   }
 }
 
-constexpr int kMaxBuf = 4;
+// Per-tile work of the interpreting kernel: switch the parameter set's
+// matrices (and flush its gradient sums) at set boundaries, then run the
+// pass's stages.
+template <int R, int NT>
+struct InterpBody {
+  const PassDesc& P;
+  const double2* mats;
+  double* grad_partials;
+  double2* smat;
+  double* gslots;
+  uint32_t sshift;
+  uint32_t cur_set;
 
-template <int N>
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-
-// NT threads per CTA, all of them compute; the lanes of warp 0 also issue the
-// TMA copies.  Tiles cycle through `nbuf` shared-memory buffers: while tile i
-// is computed, tiles up to i + depth are loading and the stores of earlier
-// tiles are draining.  depth = nbuf - 2 for nbuf >= 3, else nbuf - 1, so the
-// buffer a load re-arms always held a tile every thread has finished with, and
-// its mbarrier is armed once per phase.
-template <int R, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-    tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
-                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf,
-                     double* __restrict__ grad_partials) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar_loaded[kMaxBuf];
-  __shared__ volatile int abort_flag;
-
-  // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
-  // [gradient accumulators: one row of ngrad per octet of threads (adjoint passes)]
-  double2* tiles = reinterpret_cast<double2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const uint32_t tile_elems = 1u << P.M;
-  double2* smat = tiles + (size_t)nbuf * tile_elems;
-  const uint64_t ntiles = P.ntiles;
-  const uint64_t first = blockIdx.x;
-  // set of the tiles being processed (the CTA's tiles ascend, so each set is
-  // met in one run); its matrices sit in smat, its gradient sums in gslots
-  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
-  uint32_t cur_set = (first < ntiles) ? (uint32_t)(first >> sshift) : 0u;
-  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + i];
-  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
-  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
   // gradient partials of the current set: octet rows summed in order, one
   // column per CTA; rows the CTA never touches stay as the host zeroed them
-  auto flush_grads = [&]() {
-    for (uint32_t i = tid; i < P.ngrad; i += NT) {
+  __device__ __forceinline__ void flush_grads() {
+    for (uint32_t i = threadIdx.x; i < P.ngrad; i += NT) {
       double v = 0.0;
       for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
       grad_partials[((size_t)cur_set * P.grad_stride + P.grad_term[i]) * gridDim.x + blockIdx.x] = v;
     }
-  };
-  if (tid == 0) {
-    for (int b = 0; b < nbuf; ++b) mbar_init(&bar_loaded[b], NT / 32);   // one arrival per warp
-    abort_flag = 0;
-    fence_mbar_init();
   }
-  __syncthreads();
-
-  const uint64_t cnt = (first < ntiles) ? (ntiles - 1 - first) / gridDim.x + 1 : 0;
-  const int depth = nbuf >= 3 ? nbuf - 2 : nbuf - 1;   // < nbuf
-
-  // ---- copy issue setup: every warp issues its share of a tile's copies
-  // (issues j = warp + NW * (lane + 32 r)); the tile mbarrier expects one
-  // arrival per warp.  Coordinates are linear in the disjoint address bits, so
-  // each lane keeps the offsets of its issues and adds the tile's base
-  // coordinates per tile.
-  constexpr int NW = NT / 32;
-  const int warp = tid >> 5;
-  const int nbox = P.nbox;
-  const int nissue = 1 << (P.nH - nbox);
-  const uint32_t box_elems = 1u << (P.c + nbox);
-  const uint32_t box_bytes = box_elems * 16u;
-  constexpr int kMaxPerLane = 1;   // nissue <= 32 * NW
-  int jc1[kMaxPerLane], jc3[kMaxPerLane], jc4[kMaxPerLane], jj[kMaxPerLane];
-  uint32_t my_bytes = 0;           // bytes of this warp's issues per tile
-#pragma unroll
-  for (int r = 0; r < kMaxPerLane; ++r) {
-    const int j = warp + NW * (lane + 32 * r);
-    jj[r] = j;
-    int c2;
-    if (j < nissue) chunk_coords(issue_offset(j, P), P, jc1[r], c2, jc3[r], jc4[r]);
-    else jc1[r] = jc3[r] = jc4[r] = 0;
-  }
-  for (int j = warp; j < nissue; j += NW) my_bytes += box_bytes;
-  TileCoordMap cmap;               // tile index -> tensor-map coordinates (32-bit, per thread)
-  tile_coord_map(P, cmap);
-  auto base_coords = [&](uint64_t t, int& c1, int& c3, int& c4) {
-    int c2;
-    tile_coords((uint32_t)t, cmap, c1, c2, c3, c4);
-  };
-  auto issue_load = [&](uint64_t i) {   // whole warp, converged
-    const int b = (int)(i % nbuf);
-    int c1, c3, c4;
-    base_coords(first + i * gridDim.x, c1, c3, c4);
-    double2* buf = tiles + (size_t)b * tile_elems;
-    if (lane == 0) mbar_arrive_expect_tx(&bar_loaded[b], my_bytes);
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-      if (jj[r] < nissue)
-        tma_load_5d(buf + (size_t)jj[r] * box_elems, &tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r],
-                    &bar_loaded[b]);
-  };
-  auto issue_store = [&](uint64_t i) {  // whole warp; one bulk group per lane per tile
-    const int b = (int)(i % nbuf);
-    int c1, c3, c4;
-    base_coords(first + i * gridDim.x, c1, c3, c4);
-    double2* buf = tiles + (size_t)b * tile_elems;
-#pragma unroll
-    for (int r = 0; r < kMaxPerLane; ++r)
-      if (jj[r] < nissue)
-        tma_store_5d(&tm, 0, c1 + jc1[r], 0, c3 + jc3[r], c4 + jc4[r], buf + (size_t)jj[r] * box_elems);
-    bulk_commit();
-  };
-
-  uint64_t issued = 0;             // tiles whose loads have been issued
-  uint64_t first_unwaited = cnt;   // first tile whose load wait did not succeed
-  for (; issued < (uint64_t)depth && issued < cnt; ++issued) issue_load(issued);
-
-  for (uint64_t i = 0; i < cnt; ++i) {
-    const int b = (int)(i % nbuf);
-    // abort_flag is read after the previous iteration's barrier: uniform in the CTA
-    const bool ab = __shfl_sync(0xffffffffu, (int)abort_flag, 0) != 0;
-    if (i + depth < cnt && !ab) {
-      // buffer (i + depth) % nbuf last held tile i + depth - nbuf (finished by
-      // every thread: it is at most tile i - 1), whose store is followed by
-      // nbuf - depth - 1 later stores: wait only for that store's read
-      if (i + depth >= (uint64_t)nbuf) {
-        if (nbuf - depth - 1 >= 1) bulk_wait_read<1>();
-        else bulk_wait_read<0>();
-      }
-      __syncwarp();
-      issue_load(i + depth);
-      issued = i + depth + 1;
-    }
-    const bool ok = bounded_wait(&bar_loaded[b], (uint32_t)((i / nbuf) & 1), &abort_flag, status, DEV_WAIT_LOADED);
-    const bool work = __syncthreads_and(ok && !abort_flag);
-    if (!work && first_unwaited == cnt) first_unwaited = i;
-    const uint32_t tset = (uint32_t)((first + i * gridDim.x) >> sshift);   // uniform in the CTA
+  __device__ __forceinline__ void operator()(double2* buf, uint64_t t, bool work) {
+    const int tid = threadIdx.x;
+    const uint32_t tset = (uint32_t)(t >> sshift);   // uniform in the CTA
     if (tset != cur_set) {   // every thread is past the previous tile's stages
       if (P.ngrad) {
         flush_grads();
@@ -792,21 +560,39 @@ __global__ void __launch_bounds__(NT, MINB)
         smat[j] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + j];
       __syncthreads();
     }
-    double2* buf = tiles + (size_t)b * tile_elems;
     for (int s = 0; s < P.nstages; ++s) {
       if (work) run_stage<R>(buf, P, s, smat, tid, NT, gslots);
       __syncthreads();
     }
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (work) issue_store(i);
   }
-  // after an abort, let loads that were issued but never consumed land first
-  for (uint64_t i = first_unwaited; i < issued; ++i) drain_wait(&bar_loaded[i % nbuf], (uint32_t)((i / nbuf) & 1));
-  bulk_wait_all();
+};
+
+// The interpreting tile-pass kernel: NT threads per CTA run the pass's
+// stages (run_stage) on each tile the pipeline makes resident.
+template <int R, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
+                     const double2* __restrict__ mats, int* __restrict__ status, int nbuf,
+                     double* __restrict__ grad_partials) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
+  // [gradient accumulators: one row of ngrad per octet of threads (adjoint passes)]
+  double2* tiles = aligned_tiles(smem_raw);
+  const int tid = threadIdx.x;
+  double2* smat = tiles + (size_t)nbuf * (1u << P.M);
+  const uint64_t first = blockIdx.x;
+  // set of the tiles being processed (the CTA's tiles ascend, so each set is
+  // met in one run); its matrices sit in smat, its gradient sums in gslots
+  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
+  const uint32_t set0 = (first < P.ntiles) ? (uint32_t)(first >> sshift) : 0u;
+  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)set0 * P.set_mat_stride + i];
+  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
+  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
+  InterpBody<R, NT> body{P, mats, grad_partials, smat, gslots, sshift, set0};
+  tile_pipeline<NT>(tm, P, tiles, status, nbuf, body);
   if (P.ngrad) {   // the last set's gradient partials
     __syncthreads();
-    flush_grads();
+    body.flush_grads();
   }
 }
 

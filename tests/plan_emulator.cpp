@@ -431,3 +431,66 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
   }
   return 0;
 }
+
+// Plan `ops` as emu_apply does and write the source of every pass's
+// specialised kernel (iq_jitgen.cpp) into `out`, separated by lines
+// "//@@PASS@@".  Returns the number of sources, or -1 (message in `out`).
+extern "C" int emu_jit_sources(int nbits, int M, int c, int R, int max_stages, double budget, int fuse, int nops,
+                               const int* ks, const int* qs, const double* mats, const long long* mat_off,
+                               char* out, long long outlen) {
+  std::vector<cd> pool;
+  std::vector<SchedOp> ops;
+  for (int i = 0; i < nops; ++i) {
+    SchedOp o{};
+    o.k = (uint8_t)ks[i];
+    for (int j = 0; j < ks[i]; ++j) o.q[j] = (uint8_t)qs[i * 5 + j];
+    const int d = 1 << ks[i];
+    const double* m = mats + 2 * mat_off[i];
+    o.mat = (uint32_t)pool.size();
+    o.dense = o.mat;
+    for (int j = 0; j < d * d; ++j) pool.emplace_back(m[2 * j], m[2 * j + 1]);
+    double ph[8];
+    uint8_t perm = 0, unit = 0;
+    if (ks[i] <= 2 && classify_monomial(m, ks[i], &perm, ph, &unit)) {
+      o.mono = 1;
+      o.perm = perm;
+      o.unit = unit;
+      o.mat = (uint32_t)pool.size();
+      for (int j = 0; j < d; ++j) pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    }
+    ops.push_back(o);
+  }
+  std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(pool.data()),
+                         reinterpret_cast<const cplx64*>(pool.data()) + pool.size());
+  if (fuse) ops = fuse_two_qubit_blocks(ops, cp);
+  SchedParams p{};
+  p.nbits = nbits;
+  p.M = M;
+  p.c = c;
+  p.R = R;
+  p.max_stages = max_stages;
+  p.budget = budget;
+  std::vector<PassPlan> plans;
+  std::string err, all;
+  if (plan_passes(p, ops, plans, err) < 0) {
+    snprintf(out, (size_t)outlen, "plan: %s", err.c_str());
+    return -1;
+  }
+  std::vector<cplx64> packed;
+  pack_pass_matrices(plans, cp.data(), packed);
+  for (size_t i = 0; i < plans.size(); ++i) {
+    const std::string s = jit_pass_source(plans[i].desc, err);
+    if (s.empty()) {
+      snprintf(out, (size_t)outlen, "pass %zu: %s", i, err.c_str());
+      return -1;
+    }
+    if (i) all += "\n//@@PASS@@\n";
+    all += s;
+  }
+  if ((long long)all.size() + 1 > outlen) {
+    snprintf(out, (size_t)outlen, "output buffer too small (%zu bytes needed)", all.size() + 1);
+    return -1;
+  }
+  memcpy(out, all.c_str(), all.size() + 1);
+  return (int)plans.size();
+}

@@ -1,0 +1,115 @@
+"""Specialised pass kernels (option "jit") on the GPU: the same planned passes
+run by the generated kernels and by the interpreting kernel give identical
+amplitudes (same arithmetic expression per operation, same pipeline), and the
+oracle's within 1e-12.  Covers register slots R = 3, 4, 5, density matrices,
+recorded programs, and flushes that pick up kernels compiled in the background."""
+import numpy as np
+import pytest
+
+from tests.test_gpu_sv import apply_abi
+from tests.test_scheduler_emulated import gen_ops, oracle_apply, rand_unitary
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def B():
+    from invariantq_b200 import binding
+    return binding
+
+
+def run_sv(B, n, ops, jit, **opts):
+    sv = B.NativeStateVector(n)
+    try:
+        sv.set_option("jit", jit)
+        for k, v in opts.items():
+            sv.set_option(k, v)
+        apply_abi(sv, ops)
+        return sv.get_amplitudes(), sv.stats()
+    finally:
+        sv.close()
+
+
+@pytest.mark.parametrize("n,kmax,R,M", [(12, 4, 4, 11), (16, 2, 4, 12), (13, 3, 3, 11), (14, 5, 5, 12)])
+def test_specialised_equals_interpreting(B, port, n, kmax, R, M):
+    rng = np.random.default_rng(100 + n + R)
+    ops = gen_ops(rng, n, 120, kmax=kmax)
+    opts = {"tile_bits": M, "reg_slots": R, "budget": 96}
+    a0, s0 = run_sv(B, n, ops, 0, **opts)
+    a2, s2 = run_sv(B, n, ops, 2, **opts)
+    assert s0["jit_passes"] == 0
+    assert s2["jit_passes"] == s2["tile_passes"] > 0
+    assert np.array_equal(a0, a2)
+    ref = oracle_apply(port, port.zero_state(n), n, ops)
+    assert np.max(np.abs(a2 - ref)) < TOL
+
+
+def test_recorded_program_compiles_at_record_end(B):
+    """Default jit = 1, 20 qubits: every pass of a recorded program runs specialised."""
+    from invariantq_b200.circuits import brickwall
+    from invariantq_b200.simulator import apply_gate_matrix
+    n = 20
+    c = brickwall(n, 12, seed=5)
+    out = []
+    for jit in (0, 1):
+        sv = B.NativeStateVector(n)
+        sv.set_option("jit", jit)
+        with sv.record() as rec:
+            for op in c.ops:
+                qs = [c.get_qubit_index(q) for q in op.qubits]
+                apply_gate_matrix(sv, qs, np.asarray(op.matrix, np.complex128))
+        prog = rec.program
+        sv.reset()
+        prog.run(sv)
+        st = sv.stats()
+        out.append(sv.get_amplitudes())
+        assert st["jit_passes"] == (prog.passes if jit else 0)
+        sv.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_flushes_use_background_compiled_kernels(B):
+    """jit = 1 on 2^18 amplitudes: the first run queues its passes' kernels,
+    a run of the same structure after jit_wait uses them."""
+    n = 18
+    rng = np.random.default_rng(7)
+    ops = gen_ops(rng, n, 90, kmax=2)
+    a0, _ = run_sv(B, n, ops, 0)
+    sv = B.NativeStateVector(n)
+    try:
+        apply_abi(sv, ops)
+        first = sv.get_amplitudes()
+        assert B.jit_wait(300.0)
+        before = sv.stats()["jit_passes"]
+        sv.reset()
+        apply_abi(sv, ops)
+        again = sv.get_amplitudes()
+        assert sv.stats()["jit_passes"] > before
+    finally:
+        sv.close()
+    assert np.array_equal(first, a0) and np.array_equal(again, a0)
+    info = B.jit_info()
+    assert info["compiled"] + info["from_disk"] > 0 and info["note"] == ""
+
+
+def test_density_matrix_specialised(B):
+    n = 7
+    rng = np.random.default_rng(3)
+    mats = []
+    for jit in (0, 2):
+        dm = B.NativeDensityMatrix(n)
+        dm.set_option("jit", jit)
+        r = np.random.default_rng(3)
+        for _ in range(25):
+            a, b = (int(x) for x in r.choice(n, 2, replace=False))
+            dm.apply_1q_unitary(a, rand_unitary(r, 2))
+            dm.apply_2q_unitary(a, b, rand_unitary(r, 4))
+            p = 0.05
+            dm.apply_1q_kraus(b, [np.sqrt(1 - p) * np.eye(2), np.sqrt(p) * np.array([[0, 1], [1, 0]])])
+        mats.append(dm.get_matrix())
+        assert (dm.stats()["jit_passes"] > 0) == (jit == 2)
+        dm.close()
+    assert np.array_equal(mats[0], mats[1])
+    assert abs(np.trace(mats[1]).real - 1.0) < 1e-12
+    del rng

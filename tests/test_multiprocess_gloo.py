@@ -65,7 +65,8 @@ def emu_path(tmp_path_factory):
     out = tmp_path_factory.mktemp("emu_mp") / "libplanemu.so"
     subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-o", str(out),
                     str(REPO / "tests" / "plan_emulator.cpp"),
-                    str(REPO / "invariantq_b200" / "csrc" / "iq_sched.cpp")], check=True)
+                    str(REPO / "invariantq_b200" / "csrc" / "iq_sched.cpp"),
+                    str(REPO / "invariantq_b200" / "csrc" / "iq_jitgen.cpp")], check=True)
     return str(out)
 
 
