@@ -143,7 +143,11 @@ size_t iq_statevector_num_qubits(void* sv);
  * 0 off; 1, the default, compiles a recorded program's kernels at record_end
  * and lets flushes use kernels already compiled for their structure, queuing
  * the missing ones for compilation on background threads, for arrays of at
- * least 2^18 amplitudes; 2 compiles before every first launch, any size).
+ * least 2^18 amplitudes; 2 compiles before every first launch, any size),
+ * "plan_style" (0: follow "jit"; 1: plan for the interpreting kernel, fusing
+ * one-qubit gates into two-qubit blocks; 2: plan for specialised kernels,
+ * leaving CX/CZ/SWAP apart and normalising dense one-qubit gates), "normalize"
+ * (1: normalised one-qubit gates in plans of style 2).
  * 0 = ok, -1 = unknown key or bad value. */
 int iq_handle_set_option(void* h, const char* key, double value);
 double iq_handle_get_option(void* h, const char* key);

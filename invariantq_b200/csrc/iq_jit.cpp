@@ -52,10 +52,13 @@ const Nvrtc& nvrtc() {
   static Nvrtc n;
   static std::once_flag once;
   std::call_once(once, [] {
-    void* h = nullptr;
-    for (const char* name : {"/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so.12", "libnvrtc.so"}) {
-      h = dlopen(name, RTLD_NOW | RTLD_LOCAL);
+    // One NVRTC per process: reuse a copy already loaded (torch preloads its
+    // own with global symbol binding); a second copy loaded beside it would
+    // have its internal calls bound to the first one's exported functions.
+    void* h = dlopen("libnvrtc.so.12", RTLD_NOW | RTLD_NOLOAD);
+    for (const char* name : {"libnvrtc.so.12", "/usr/local/cuda/lib64/libnvrtc.so.12"}) {
       if (h) break;
+      h = dlopen(name, RTLD_NOW | RTLD_LOCAL | RTLD_DEEPBIND);
     }
     if (!h) { n.why = "libnvrtc.so.12 not found"; return; }
     auto get = [&](const char* s) { return dlsym(h, s); };
@@ -193,7 +196,10 @@ struct JitKernel {
 namespace {
 
 // Compiled kernels by (device, source), the sources queued for background
-// compilation, and the worker threads that compile them.
+// compilation, and the worker threads that compile them.  Never destroyed: at
+// exit an atexit handler empties the queue and waits (bounded) for the
+// compilations in progress; idle workers stay parked on the condition
+// variable, which outlives them.
 struct JitState {
   std::mutex mu;
   std::condition_variable cv, idle;
@@ -204,21 +210,20 @@ struct JitState {
   int busy = 0;
   bool stop = false;
   std::string last_error;
-
-  ~JitState() {
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      stop = true;
-      queue.clear();
-    }
-    cv.notify_all();
-    for (auto& t : workers) t.join();
-  }
 };
 
 JitState& state() {
-  static JitState s;
-  return s;
+  static JitState* s = new JitState;
+  return *s;
+}
+
+void drain_at_exit() {
+  JitState& S = state();
+  std::unique_lock<std::mutex> lk(S.mu);
+  S.stop = true;
+  for (auto& k : S.queue) S.pending.erase(k);
+  S.queue.clear();
+  S.idle.wait_for(lk, std::chrono::seconds(60), [&] { return S.busy == 0; });
 }
 
 std::string cubin_path(const std::string& dir, const std::string& src) {
@@ -271,8 +276,9 @@ void worker_loop() {
     std::pair<int, std::string> task;
     {
       std::unique_lock<std::mutex> lk(S.mu);
-      S.cv.wait(lk, [&] { return S.stop || !S.queue.empty(); });
-      if (S.stop) return;
+      // after stop (process exit) the worker stays parked here: returning would
+      // run its thread-local teardown while the process is tearing down
+      S.cv.wait(lk, [&] { return !S.stop && !S.queue.empty(); });
       task = std::move(S.queue.front());
       S.queue.pop_front();
       ++S.busy;
@@ -310,7 +316,8 @@ bool jit_ready(std::string& err, int& dev) {
 
 }  // namespace
 
-bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err) {
+bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
+                 int min_blocks) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   if (!jit_ready(err, dev)) return false;
@@ -322,7 +329,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      srcs[i] = jit_pass_source(*passes[i], e);
+      srcs[i] = jit_pass_source(*passes[i], e, min_blocks);
       if (srcs[i].empty()) continue;
       auto it = S.cache.find({dev, srcs[i]});
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
@@ -354,7 +361,8 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
   return true;
 }
 
-void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing) {
+void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
+                int min_blocks) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   std::string err;
@@ -365,7 +373,7 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      std::string src = jit_pass_source(*passes[i], e);
+      std::string src = jit_pass_source(*passes[i], e, min_blocks);
       if (src.empty()) continue;
       std::pair<int, std::string> key(dev, std::move(src));
       auto it = S.cache.find(key);
@@ -376,9 +384,20 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
       queued = true;
     }
     if (queued && S.workers.empty()) {
+      // NVRTC sets up (and registers the teardown of) its compiler state on
+      // its first compilation.  Compile once here, on this thread, before the
+      // exit handler that drains the workers is registered: exit handlers run
+      // in reverse order, so the drain then runs before NVRTC's teardown and
+      // no compilation is in flight when NVRTC's state goes away.
+      std::string cubin, werr;
+      compile_cubin("extern \"C\" __global__ void iq_jit_warmup() {}\n", cubin, werr);
+      atexit(drain_at_exit);
       const unsigned hw = std::thread::hardware_concurrency();
       const int n = (int)std::max(1u, std::min(hw ? hw / 2 : 1u, 16u));
-      for (int t = 0; t < n; ++t) S.workers.emplace_back(worker_loop);
+      for (int t = 0; t < n; ++t) {
+        S.workers.emplace_back(worker_loop);
+        S.workers.back().detach();
+      }
     }
   }
   if (queued) S.cv.notify_all();

@@ -31,12 +31,16 @@ struct JitKernel;
 // parallel.  out[i] is null for a pass that is not specialised.  Returns false
 // (with `err`) when NVRTC or the driver entry points are unavailable or a
 // compile fails.
-bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err);
+// min_blocks: resident CTAs per SM the kernels are compiled for (the launch's
+// TileLaunch::ctas_per_sm).
+bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
+                 int min_blocks);
 
 // Kernels already compiled for these passes (null where none); with
 // queue_missing, the missing ones are queued for compilation on background
 // threads, so a later plan with the same structure finds them.
-void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing);
+void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
+                int min_blocks);
 
 // Wait (at most timeout_s) until the background compilations have finished.
 bool jit_wait(double timeout_s);

@@ -67,6 +67,17 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         }
         break;
       }
+      case OP_N1R: {   // row 0's entry in column perm is exactly 1
+        const int A = 1 << od.a;
+        for (int v = 0; v < NV; ++v) {
+          if (v & A) continue;
+          const std::string x = cur[v], y = cur[v | A];
+          cur[v] = od.perm ? def("cfma(" + y + ", " + mat(m + 0) + ", " + x + ")")
+                           : def("cfma(" + x + ", " + mat(m + 1) + ", " + y + ")");
+          cur[v | A] = def("cfma(cmul(" + mat(m + 2) + ", " + x + "), " + mat(m + 3) + ", " + y + ")");
+        }
+        break;
+      }
       case OP_M1R: {
         const int A = 1 << od.a;
         const bool sw = od.perm & 1;
@@ -166,7 +177,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
 }  // namespace
 
 // Source of the kernel specialised to pass `d` (see iq_plan.h).
-std::string jit_pass_source(const PassDesc& d, std::string& err) {
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks) {
   if (d.ngrad || d.nsets > 1) {
     err = "adjoint passes are not specialised";
     return "";
@@ -176,7 +187,7 @@ std::string jit_pass_source(const PassDesc& d, std::string& err) {
     return "";
   }
   const int NT = tile_pass_threads(d.R);
-  const int MINB = d.R == 5 ? 1 : 2;
+  const int MINB = d.R == 5 ? 1 : (min_blocks >= 1 && min_blocks <= 4 ? min_blocks : 2);
   const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
   Gen g;
   std::ostringstream& o = g.o;

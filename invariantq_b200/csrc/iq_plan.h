@@ -71,6 +71,9 @@ enum OpKind : uint8_t {
                 // `gidx`, then apply the 2x2 matrix at `mat` to the qubit for both halves; the
                 // matrix is the inverse rotation exp(+i t P / 2) and is read through its
                 // structure (entries 0, 1, 3)
+  OP_N1R = 9,   // one-qubit 2x2 on register slot a whose row-0 entry in column `perm`
+                // (0 or 1) is exactly 1: that product is skipped (6 instead of 8 FMAs per
+                // amplitude); the matrix is stored whole, so a lane placement runs it as OP_D1L
 };
 
 // flags
@@ -129,6 +132,7 @@ struct SchedOp {
   uint8_t unit;          // monomial with unit phases
   uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
   uint32_t dense;        // complex offset of the dense 2^k x 2^k matrix (always present)
+  uint8_t norm;          // k = 1 dense, normalised: row-0 entry in column norm - 1 is exactly 1 (0: not)
   uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
   uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
   uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
@@ -299,13 +303,28 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 // layout, operations and matrix offsets fixed; tile bits, tile count and
 // matrix values stay launch parameters.  Returns "" and sets `err` for a pass
 // that is not specialised (adjoint steps, several parameter sets).
-std::string jit_pass_source(const PassDesc& d, std::string& err);
+// min_blocks: resident CTAs per SM the kernel's register budget is sized for
+// (launch bounds; 2 when out of 1..4; always 1 for R = 5).
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2);
 struct cplx64 { double re, im; };
 // Fuse runs of queued operations on at most two qubits into single 4x4 blocks
 // (a two-qubit operation absorbs the open one-qubit blocks of its qubits and
 // later one-qubit operations on them), appending the fused matrices to `pool`.
 // Operation order per qubit is preserved.  Returns the fused list.
-std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool);
+// With monomial_barrier, two-qubit monomials (CX, CZ, SWAP: free renamings or
+// phase products in the specialised kernels) are left alone and end the
+// one-qubit runs of their qubits.
+std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool,
+                                           bool monomial_barrier = false);
+// Divide every dense one-qubit operation but the last of each run of at most
+// kNormSegment by the larger of its row-0 entries (marking it `norm`), and
+// multiply the run's last one by the product of those divisors: a scalar
+// factor commutes with every operation, so the state after the run's last
+// operation is unchanged, while each normalised operation costs 6 FMAs per
+// amplitude instead of 8.  Runs are bounded so the scale of the intermediate
+// state stays within (1/sqrt 2)^kNormSegment of the true one.
+constexpr int kNormSegment = 256;
+void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool);
 // Re-pack the matrix data each pass references (absolute offsets into `pool`)
 // into one contiguous block per pass: sets desc.mat_base / mat_elems and makes
 // every op's `mat` relative to its pass block, which the kernel stages in

@@ -212,6 +212,8 @@ struct Engine {
   // 2^kJitMinBits amplitudes; 2 both compiled before their first launch, any size.
   int jit = 1;
   static constexpr int kJitMinBits = 18;
+  int normalize = 1;   // normalised one-qubit operations in specialised passes
+  int plan_style = 0;  // 0: by the jit setting; 1: as for the interpreting kernel; 2: as for specialised kernels
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
 
   double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0, st_h2d = 0;
@@ -259,7 +261,7 @@ struct Engine {
     sp.c = env_int("IQ_CHUNK_BITS", 5);
     sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));   // register slots (R); wider blocks raise it
     sp.max_stages = env_int("IQ_MAX_STAGES", 8);
-    sp.budget = env_double("IQ_PASS_BUDGET", 80.0);
+    sp.budget = env_double("IQ_PASS_BUDGET", 120.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
     tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
     eager = env_int("IQ_EAGER", 0);
@@ -404,12 +406,12 @@ struct Engine {
     for (auto& pl : pg.plans) ds.push_back(&pl.desc);
     if (own || jit >= 2) {
       std::string err;
-      if (!jit_prepare(ds, pg.jit, err)) {
+      if (!jit_prepare(ds, pg.jit, err, tl.ctas_per_sm)) {
         jit_note(err);
         pg.jit.clear();
       }
     } else {
-      jit_lookup(ds, pg.jit, true);
+      jit_lookup(ds, pg.jit, true, tl.ctas_per_sm);
     }
     bool any = false;
     for (auto* k : pg.jit) any |= k != nullptr;
@@ -419,7 +421,12 @@ struct Engine {
 
   bool build_program(Program& pg, bool own) {
     pg.nops = (int)ops.size();
-    const std::vector<SchedOp> fused = fuse ? fuse_two_qubit_blocks(ops, pool) : ops;
+    // passes that specialised kernels will run: two-qubit monomials stay apart
+    // (renamings there) and dense one-qubit operations are normalised
+    const bool spec = plan_style == 2 ||
+                      (plan_style == 0 && jit && (jit >= 2 || nbits >= kJitMinBits) && !eager && nbits >= 7);
+    std::vector<SchedOp> fused = fuse ? fuse_two_qubit_blocks(ops, pool, spec) : ops;
+    if (spec && normalize) normalize_one_qubit_ops(fused, pool);
     int maxk = 1;
     for (auto& o : fused) maxk = std::max<int>(maxk, o.k);
     pg.tiled = !eager && nbits >= 7;
@@ -1117,6 +1124,8 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "flush_ops")) { if (iv < 1) return -1; e->flush_ops = iv; }
   else if (!strcmp(key, "profile")) e->profile = iv ? 1 : 0;
   else if (!strcmp(key, "jit")) { if (iv < 0 || iv > 2) return -1; e->jit = iv; }
+  else if (!strcmp(key, "normalize")) e->normalize = iv ? 1 : 0;
+  else if (!strcmp(key, "plan_style")) { if (iv < 0 || iv > 2) return -1; e->plan_style = iv; }
   else if (!strcmp(key, "inject_status")) {   // failure-path tests: as if a tile pass had timed out
     if (iv < 1 || iv > 2) return -1;
     if (!cuda_ok(cudaMemcpyAsync(e->d_status, &iv, sizeof(int), cudaMemcpyHostToDevice, e->stream), "inject status") ||
@@ -1143,6 +1152,8 @@ double iq_handle_get_option(void* h, const char* key) {
   if (!strcmp(key, "flush_ops")) return e->flush_ops;
   if (!strcmp(key, "profile")) return e->profile;
   if (!strcmp(key, "jit")) return e->jit;
+  if (!strcmp(key, "normalize")) return e->normalize;
+  if (!strcmp(key, "plan_style")) return e->plan_style;
   return kNaN;
 }
 

@@ -29,6 +29,7 @@ int op_mat_elems(const SchedOp& op) {
 double op_cost(const SchedOp& op, double grad_cost) {
   if (op.grad) return grad_cost;   // 2x2 on both halves plus the gradient products
   if (op.mono) return op.unit ? 0.25 : 4.0;
+  if (op.norm) return 6.0;
   return 4.0 * double(1u << op.k);
 }
 
@@ -415,7 +416,11 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         od.flags = o.unit ? OPF_UNIT_PHASE : 0;
         if (o.k == 1) {
           const int j = pos[o.q[0]];
-          if (slot_of[j] >= 0) { od.kind = o.mono ? OP_M1R : OP_D1R; od.a = (uint8_t)slot_of[j]; }
+          if (slot_of[j] >= 0) {
+            od.kind = o.mono ? OP_M1R : (o.norm ? OP_N1R : OP_D1R);
+            od.a = (uint8_t)slot_of[j];
+            if (o.norm) od.perm = (uint8_t)(o.norm - 1);
+          }
           else if (lane_of[j] >= 0) { od.kind = o.mono ? OP_M1L : OP_D1L; od.a = (uint8_t)lane_of[j]; }
           else { err = "internal: 1q operation bit is neither a slot nor a lane"; return -1; }
         } else if (o.k == 2) {
@@ -498,7 +503,8 @@ struct Block {
 
 }  // namespace
 
-std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool) {
+std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std::vector<cplx64>& pool,
+                                           bool monomial_barrier) {
   const int nb = 64;
   std::vector<Block> blocks;
   std::vector<int> open(nb, -1), last(nb, -1);
@@ -511,7 +517,9 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
   };
   for (size_t i = 0; i < ops.size(); ++i) {
     const SchedOp& o = ops[i];
-    if (o.k >= 3 || o.grad) {   // wide blocks and adjoint steps pass through unchanged
+    // wide blocks and adjoint steps pass through unchanged, and so do two-qubit
+    // monomials (CX, CZ, SWAP) when they are cheaper alone than inside a 4x4
+    if (o.k >= 3 || o.grad || (monomial_barrier && o.k == 2 && o.mono)) {
       for (int j = 0; j < o.k; ++j) { open[o.q[j]] = -1; last[o.q[j]] = (int)blocks.size(); }
       Block b;
       b.k = 0;
@@ -634,6 +642,34 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
     out.push_back(o);
   }
   return out;
+}
+
+void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool) {
+  std::vector<int> dense1;
+  for (size_t i = 0; i < ops.size(); ++i)
+    if (ops[i].k == 1 && !ops[i].mono && !ops[i].grad) dense1.push_back((int)i);
+  for (size_t s0 = 0; s0 < dense1.size(); s0 += kNormSegment) {
+    const size_t s1 = std::min(dense1.size(), s0 + kNormSegment);
+    if (s1 - s0 < 2) break;
+    cplx64 scale{1.0, 0.0};
+    for (size_t j = s0; j + 1 < s1; ++j) {
+      SchedOp& o = ops[dense1[j]];
+      const cplx64* U = pool.data() + o.dense;
+      const int col = (std::hypot(U[1].re, U[1].im) > std::hypot(U[0].re, U[0].im)) ? 1 : 0;
+      const cplx64 s = U[col];
+      const double n2 = s.re * s.re + s.im * s.im;
+      const cplx64 inv{s.re / n2, -s.im / n2};
+      const uint32_t at = (uint32_t)pool.size();
+      for (int e = 0; e < 4; ++e) pool.push_back(e == col ? cplx64{1.0, 0.0} : cm(pool[o.dense + e], inv));
+      o.dense = o.mat = at;
+      o.norm = (uint8_t)(col + 1);
+      scale = cm(scale, s);
+    }
+    SchedOp& c = ops[dense1[s1 - 1]];   // the run's carrier takes the product of the divisors
+    const uint32_t at = (uint32_t)pool.size();
+    for (int e = 0; e < 4; ++e) pool.push_back(cm(pool[c.dense + e], scale));
+    c.dense = c.mat = at;
+  }
 }
 
 // ------------------------------------------------------------ adjoint builder

@@ -68,6 +68,19 @@ __device__ __forceinline__ void d1r(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
+// normalised 2x2 (OP_N1R): row 0's entry in column COL is exactly 1
+template <int R, int S, int COL>
+__device__ __forceinline__ void n1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
+  const double2 u = ld_mat(m, 1 - COL), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & (1 << S)) continue;
+    const double2 x = s[v], y = s[v | (1 << S)];
+    d[v] = COL == 0 ? cfma(x, u, y) : cfma(y, u, x);
+    d[v | (1 << S)] = cfma(cmul(u2, x), u3, y);
+  }
+}
+
 template <int R, int S, bool SW, bool UNIT>
 __device__ __forceinline__ void m1r_t(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
   double2 p0 = make_double2(1.0, 0.0), p1 = p0;
@@ -336,6 +349,18 @@ __device__ __forceinline__ void disp_d1r(int sl, const double2 (&s)[1 << R], dou
   }
 }
 template <int R, int S = 0>
+__device__ __forceinline__ void disp_n1r(int sl, int col, const double2 (&s)[1 << R], double2 (&d)[1 << R],
+                                         const double2* m) {
+  if constexpr (S < R) {
+    if (sl == S) {
+      if (col) n1r<R, S, 1>(s, d, m);
+      else n1r<R, S, 0>(s, d, m);
+    } else {
+      disp_n1r<R, S + 1>(sl, col, s, d, m);
+    }
+  }
+}
+template <int R, int S = 0>
 __device__ __forceinline__ void disp_m1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
                                          int perm, bool unit) {
   if constexpr (S < R) {
@@ -429,6 +454,7 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
       break;
     }
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
+    case OP_N1R: disp_n1r<R>(od.a, od.perm, s, d, m); break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
     case OP_D2R:
       // one jump over the ordered slot pair (a, b) instead of nested compares

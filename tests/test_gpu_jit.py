@@ -1,7 +1,8 @@
 """Specialised pass kernels (option "jit") on the GPU: the same planned passes
-run by the generated kernels and by the interpreting kernel give identical
-amplitudes (same arithmetic expression per operation, same pipeline), and the
-oracle's within 1e-12.  Covers register slots R = 3, 4, 5, density matrices,
+(plan_style 2: CX/CZ/SWAP left apart, normalised one-qubit gates) run by the
+generated kernels and by the interpreting kernel give identical amplitudes
+(same arithmetic expression per operation, same pipeline), and the oracle's
+within 1e-12.  Covers register slots R = 3, 4, 5, density matrices,
 recorded programs, and flushes that pick up kernels compiled in the background."""
 import numpy as np
 import pytest
@@ -35,7 +36,7 @@ def run_sv(B, n, ops, jit, **opts):
 def test_specialised_equals_interpreting(B, port, n, kmax, R, M):
     rng = np.random.default_rng(100 + n + R)
     ops = gen_ops(rng, n, 120, kmax=kmax)
-    opts = {"tile_bits": M, "reg_slots": R, "budget": 96}
+    opts = {"tile_bits": M, "reg_slots": R, "budget": 96, "plan_style": 2}
     a0, s0 = run_sv(B, n, ops, 0, **opts)
     a2, s2 = run_sv(B, n, ops, 2, **opts)
     assert s0["jit_passes"] == 0
@@ -55,6 +56,7 @@ def test_recorded_program_compiles_at_record_end(B):
     for jit in (0, 1):
         sv = B.NativeStateVector(n)
         sv.set_option("jit", jit)
+        sv.set_option("plan_style", 2)
         with sv.record() as rec:
             for op in c.ops:
                 qs = [c.get_qubit_index(q) for q in op.qubits]
@@ -88,7 +90,8 @@ def test_flushes_use_background_compiled_kernels(B):
         assert sv.stats()["jit_passes"] > before
     finally:
         sv.close()
-    assert np.array_equal(first, a0) and np.array_equal(again, a0)
+    assert np.array_equal(first, again)            # same plan: interpreting, then specialised
+    assert np.max(np.abs(again - a0)) < TOL       # a0: planned for the interpreting kernel
     info = B.jit_info()
     assert info["compiled"] + info["from_disk"] > 0 and info["note"] == ""
 
@@ -100,6 +103,7 @@ def test_density_matrix_specialised(B):
     for jit in (0, 2):
         dm = B.NativeDensityMatrix(n)
         dm.set_option("jit", jit)
+        dm.set_option("plan_style", 2)
         r = np.random.default_rng(3)
         for _ in range(25):
             a, b = (int(x) for x in r.choice(n, 2, replace=False))
@@ -113,3 +117,19 @@ def test_density_matrix_specialised(B):
     assert np.array_equal(mats[0], mats[1])
     assert abs(np.trace(mats[1]).real - 1.0) < 1e-12
     del rng
+
+
+def test_normalised_planning_vs_oracle(B, port):
+    """Plan style 2 on the interpreting kernel, more dense one-qubit gates than
+    one normalisation run (a CZ after each keeps them from merging)."""
+    from tests.test_scheduler_emulated import CZ
+    n = 11
+    rng = np.random.default_rng(5)
+    ops = []
+    for _ in range(600):
+        q = int(rng.integers(n))
+        ops += [("1q", [q], rand_unitary(rng, 2)), ("2q", [q, (q + 1) % n], CZ)]
+    ref = oracle_apply(port, port.zero_state(n), n, ops)
+    for jit in (0, 2):
+        a, st = run_sv(B, n, ops, jit, plan_style=2)
+        assert np.max(np.abs(a - ref)) < TOL

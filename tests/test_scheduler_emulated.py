@@ -141,7 +141,8 @@ def test_emulated_passes_match_oracle(port, emu, n, M, c, R, stages, budget, see
     start = ref.copy()
     ref = oracle_apply(port, ref, n, ops)
     lsb = [to_lsb(*o) for o in ops]
-    for fuse in (0, 1):
+    # fuse 2: the specialised kernels' planning (CX/CZ/SWAP apart, normalised one-qubit gates)
+    for fuse in (0, 1, 2):
         got, npasses, per = run_emu(emu, n, lsb, start, M=M, c=c, R=R, max_stages=stages, budget=budget, fuse=fuse)
         assert per.sum() <= len(ops)
         assert fuse or per.sum() == len(ops)
@@ -168,10 +169,30 @@ def test_brickwall_pass_count_and_parity(port, emu):
     ref[0] = 1
     start = ref.copy()
     ref = oracle_apply(port, ref, n, ops)
-    got, npasses, per = run_emu(emu, n, [to_lsb(*o) for o in ops], start, M=12, c=5)
+    for fuse in (1, 2):
+        got, npasses, per = run_emu(emu, n, [to_lsb(*o) for o in ops], start, M=12, c=5, fuse=fuse)
+        assert np.max(np.abs(got - ref)) < 1e-12
+        # far fewer passes than gates
+        assert npasses < len(ops) / 4
+
+
+def test_normalisation_segments_keep_scale(port, emu):
+    """More dense one-qubit gates than one normalisation run (kNormSegment =
+    256): every run's carrier restores the scale before the state is read."""
+    n = 9
+    rng = np.random.default_rng(21)
+    ops = []
+    for _ in range(700):   # a CZ after every gate keeps the one-qubit gates from merging
+        q = int(rng.integers(n))
+        ops += [("1q", [q], rand_unitary(rng, 2)), ("2q", [q, (q + 1) % n], CZ)]
+    ops += [("2q", [0, 5], CX), ("1q", [3], rand_unitary(rng, 2))]
+    ref = np.zeros(1 << n, np.complex128)
+    ref[0] = 1
+    start = ref.copy()
+    ref = oracle_apply(port, ref, n, ops)
+    got, npasses, per = run_emu(emu, n, [to_lsb(*o) for o in ops], start, M=9, c=5, budget=1e9, fuse=2)
     assert np.max(np.abs(got - ref)) < 1e-12
-    # far fewer passes than gates
-    assert npasses < len(ops) / 4
+    assert abs(np.linalg.norm(got) - 1.0) < 1e-12
 
 
 @pytest.mark.parametrize("R", [3, 4])
