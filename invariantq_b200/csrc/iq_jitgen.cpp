@@ -42,10 +42,22 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
   o << "        unsigned base = lo";
   for (int i = 0; i < sd.nt; ++i) o << " | ((((unsigned)u >> " << i << ") & 1u) << " << (int)sd.tb[i] << ")";
   o << ";\n        base = swz(base);\n";
+  // The swizzle only mixes bits 0..2: swz(base) ^ off = (swz(base) ^ (off & 7))
+  // + (off & ~7), because above bit 2 the thread's and the slots' bits are
+  // disjoint.  One pointer per distinct (off & 7) then reaches every register's
+  // slot with a constant displacement.
+  std::string ptr[8];
+  for (int v = 0; v < NV; ++v) {
+    const uint32_t k = voffc(v) & 7u;
+    if (!ptr[k].empty()) continue;
+    ptr[k] = "p" + std::to_string(k);
+    o << "        double2* const " << ptr[k] << " = tile + (base ^ " << k << "u);\n";
+  }
+  auto at = [&](int v) { return ptr[voffc(v) & 7u] + "[" + std::to_string(voffc(v) & ~7u) + "]"; };
   std::vector<std::string> cur(NV);
   for (int v = 0; v < NV; ++v) {
     cur[v] = g.fresh();
-    o << "        const double2 " << cur[v] << " = tile[base ^ " << voffc(v) << "u];\n";
+    o << "        const double2 " << cur[v] << " = " << at(v) << ";\n";
   }
   auto def = [&](const std::string& expr) {
     const std::string n = g.fresh();
@@ -169,7 +181,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         return false;
     }
   }
-  for (int v = 0; v < NV; ++v) o << "        tile[base ^ " << voffc(v) << "u] = " << cur[v] << ";\n";
+  for (int v = 0; v < NV; ++v) o << "        " << at(v) << " = " << cur[v] << ";\n";
   o << "      }\n    }\n    __syncthreads();\n";
   return true;
 }
