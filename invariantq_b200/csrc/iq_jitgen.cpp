@@ -90,6 +90,18 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         }
         break;
       }
+      case OP_R1R: {   // normalised real rotation
+        const int A = 1 << od.a;
+        const std::string w = od.perm ? mat(m + 0) + ".x" : mat(m + 2) + ".x";
+        const std::string F = od.perm ? "1" : "0";
+        for (int v = 0; v < NV; ++v) {
+          if (v & A) continue;
+          const std::string x = cur[v], y = cur[v | A];
+          cur[v] = def("rot_row0<" + F + ">(" + w + ", " + x + ", " + y + ")");
+          cur[v | A] = def("rot_row1<" + F + ">(" + w + ", " + x + ", " + y + ")");
+        }
+        break;
+      }
       case OP_M1R: {
         const int A = 1 << od.a;
         const bool sw = od.perm & 1;
@@ -97,9 +109,10 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
           if (v & A) continue;
           std::string x = cur[v], y = cur[v | A];
           if (sw) std::swap(x, y);
+          // rows whose phase is exactly 1 skip the product (same value as multiplying by 1)
           if (!unit) {
-            x = def("cmul(" + mat(m + 0) + ", " + x + ")");
-            y = def("cmul(" + mat(m + 1) + ", " + y + ")");
+            if (!(od.urows & 1)) x = def("cmul(" + mat(m + 0) + ", " + x + ")");
+            if (!(od.urows & 2)) y = def("cmul(" + mat(m + 1) + ", " + y + ")");
           }
           cur[v] = x;
           cur[v | A] = y;
@@ -158,7 +171,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
           const std::string x[4] = {cur[idx[0]], cur[idx[1]], cur[idx[2]], cur[idx[3]]};
           for (int r = 0; r < 4; ++r) {
             const std::string y = x[(od.perm >> (2 * r)) & 3];
-            cur[idx[r]] = unit ? y : def("cmul(" + mat(m + r) + ", " + y + ")");
+            cur[idx[r]] = (unit || ((od.urows >> r) & 1)) ? y : def("cmul(" + mat(m + r) + ", " + y + ")");
           }
         }
         break;

@@ -140,6 +140,19 @@ __device__ __forceinline__ bool bounded_wait(uint64_t* bar, uint32_t parity, vol
 }
 
 
+// rows of a normalised real rotation (OP_R1R) applied to the pair (x, y):
+// FORM 0 [[1, -w], [w, 1]], FORM 1 [[w, -1], [1, w]]
+template <int FORM>
+__device__ __forceinline__ double2 rot_row0(double w, double2 x, double2 y) {
+  return FORM == 0 ? make_double2(fma(-w, y.x, x.x), fma(-w, y.y, x.y))
+                   : make_double2(fma(w, x.x, -y.x), fma(w, x.y, -y.y));
+}
+template <int FORM>
+__device__ __forceinline__ double2 rot_row1(double w, double2 x, double2 y) {
+  return FORM == 0 ? make_double2(fma(w, x.x, y.x), fma(w, x.y, y.y))
+                   : make_double2(fma(w, y.x, x.x), fma(w, y.y, x.y));
+}
+
 __device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
   return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
 }

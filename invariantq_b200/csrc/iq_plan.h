@@ -74,6 +74,9 @@ enum OpKind : uint8_t {
   OP_N1R = 9,   // one-qubit 2x2 on register slot a whose row-0 entry in column `perm`
                 // (0 or 1) is exactly 1: that product is skipped (6 instead of 8 FMAs per
                 // amplitude); the matrix is stored whole, so a lane placement runs it as OP_D1L
+  OP_R1R = 10,  // real rotation on register slot a, normalised (2 FMAs per amplitude): perm 0:
+                // [[1, -t], [t, 1]] with t = Re m[2]; perm 1: [[u, -1], [1, u]] with u = Re m[0];
+                // stored whole, so a lane placement runs it as OP_D1L
 };
 
 // flags
@@ -84,7 +87,8 @@ struct OpDesc {          // 16 bytes
   uint8_t a, b, k;
   uint8_t perm;          // monomial: row r reads column (perm >> (2r)) & 3 (1q: bit 0 = swap)
   uint8_t flags;
-  uint8_t pad0, pad1;
+  uint8_t urows;         // monomial: bit r set = row r's phase is exactly 1 (its product is skipped)
+  uint8_t pad1;
   uint32_t mat;          // offset (complex elements) into the flush's matrix buffer
   uint32_t gidx;         // OP_GRAD2: the pass's local gradient index (global term: PassDesc::grad_term)
 };
@@ -133,6 +137,8 @@ struct SchedOp {
   uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
   uint32_t dense;        // complex offset of the dense 2^k x 2^k matrix (always present)
   uint8_t norm;          // k = 1 dense, normalised: row-0 entry in column norm - 1 is exactly 1 (0: not)
+  uint8_t rot;           // k = 1 real rotation, normalised: 1 = tan form, 2 = cot form (0: not)
+  uint8_t urows;         // monomial: bit r = row r's phase is exactly 1
   uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
   uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
   uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
@@ -325,6 +331,17 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
 // state stays within (1/sqrt 2)^kNormSegment of the true one.
 constexpr int kNormSegment = 256;
 void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool);
+// Factor every unitary dense one-qubit operation as diag(d0, d1) R diag(1, e1)
+// with R a real rotation (normalised: 2 FMAs per amplitude) and carry each
+// qubit's pending output diagonal forward: through diagonal and permutation
+// operations (a two-qubit monomial takes the pending diagonals of its qubits
+// and passes on whatever factors per qubit; the rest becomes a phase on its
+// |11> row), into the next dense operation on the qubit (columns scaled, no
+// cost).  What cannot be carried is emitted as one-qubit phase operations
+// diag(1, p) (2 FMAs per amplitude).  Scalars collect into runs of at most
+// kNormSegment rotations, each ended by a scalar operation.  Non-unitary
+// one-qubit matrices are left dense.
+void decompose_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool);
 // Re-pack the matrix data each pass references (absolute offsets into `pool`)
 // into one contiguous block per pass: sets desc.mat_base / mat_elems and makes
 // every op's `mat` relative to its pass block, which the kernel stages in

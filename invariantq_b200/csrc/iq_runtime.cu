@@ -426,7 +426,10 @@ struct Engine {
     const bool spec = plan_style == 2 ||
                       (plan_style == 0 && jit && (jit >= 2 || nbits >= kJitMinBits) && !eager && nbits >= 7);
     std::vector<SchedOp> fused = fuse ? fuse_two_qubit_blocks(ops, pool, spec) : ops;
-    if (spec && normalize) normalize_one_qubit_ops(fused, pool);
+    if (spec && normalize) {
+      decompose_one_qubit_ops(fused, pool);
+      normalize_one_qubit_ops(fused, pool);
+    }
     int maxk = 1;
     for (auto& o : fused) maxk = std::max<int>(maxk, o.k);
     pg.tiled = !eager && nbits >= 7;

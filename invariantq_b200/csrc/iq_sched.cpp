@@ -28,7 +28,13 @@ int op_mat_elems(const SchedOp& op) {
 
 double op_cost(const SchedOp& op, double grad_cost) {
   if (op.grad) return grad_cost;   // 2x2 on both halves plus the gradient products
-  if (op.mono) return op.unit ? 0.25 : 4.0;
+  if (op.mono) {
+    if (op.unit) return 0.25;
+    const int rows = 1 << op.k;
+    const int nonunit = rows - __builtin_popcount(op.urows & ((1u << rows) - 1));
+    return 4.0 * nonunit / rows;
+  }
+  if (op.rot) return 2.0;
   if (op.norm) return 6.0;
   return 4.0 * double(1u << op.k);
 }
@@ -414,12 +420,14 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         od.mat = o.mat;
         od.perm = o.perm;
         od.flags = o.unit ? OPF_UNIT_PHASE : 0;
+        od.urows = o.mono ? o.urows : 0;
         if (o.k == 1) {
           const int j = pos[o.q[0]];
           if (slot_of[j] >= 0) {
-            od.kind = o.mono ? OP_M1R : (o.norm ? OP_N1R : OP_D1R);
+            od.kind = o.mono ? OP_M1R : (o.rot ? OP_R1R : (o.norm ? OP_N1R : OP_D1R));
             od.a = (uint8_t)slot_of[j];
             if (o.norm) od.perm = (uint8_t)(o.norm - 1);
+            if (o.rot) od.perm = (uint8_t)(o.rot - 1);
           }
           else if (lane_of[j] >= 0) { od.kind = o.mono ? OP_M1L : OP_D1L; od.a = (uint8_t)lane_of[j]; }
           else { err = "internal: 1q operation bit is neither a slot nor a lane"; return -1; }
@@ -647,7 +655,7 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
 void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool) {
   std::vector<int> dense1;
   for (size_t i = 0; i < ops.size(); ++i)
-    if (ops[i].k == 1 && !ops[i].mono && !ops[i].grad) dense1.push_back((int)i);
+    if (ops[i].k == 1 && !ops[i].mono && !ops[i].grad && !ops[i].rot) dense1.push_back((int)i);
   for (size_t s0 = 0; s0 < dense1.size(); s0 += kNormSegment) {
     const size_t s1 = std::min(dense1.size(), s0 + kNormSegment);
     if (s1 - s0 < 2) break;
@@ -670,6 +678,222 @@ void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& poo
     for (int e = 0; e < 4; ++e) pool.push_back(cm(pool[c.dense + e], scale));
     c.dense = c.mat = at;
   }
+}
+
+namespace {
+
+inline cplx64 cdiv(cplx64 a, cplx64 b) {
+  const double n = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / n, (a.im * b.re - a.re * b.im) / n};
+}
+inline double cabs2(cplx64 a) { return a.re * a.re + a.im * a.im; }
+inline bool is_one(cplx64 a) { return a.re == 1.0 && a.im == 0.0; }
+
+struct Decomposer {
+  std::vector<SchedOp>& out;
+  std::vector<cplx64>& pool;
+  std::vector<cplx64> pa, pb;   // pending output diagonal diag(pa[q], pb[q]) of each qubit
+  cplx64 G{1.0, 0.0};           // scalar factored out of the emitted operations
+
+  Decomposer(std::vector<SchedOp>& o, std::vector<cplx64>& p) : out(o), pool(p), pa(64, {1.0, 0.0}), pb(64, {1.0, 0.0}) {}
+
+  uint32_t put(std::initializer_list<cplx64> v) {
+    const uint32_t at = (uint32_t)pool.size();
+    for (const cplx64& x : v) pool.push_back(x);
+    return at;
+  }
+  // one-qubit diagonal diag(a, b) = a diag(1, b / a): the scalar goes to G
+  void emit_phase(int q, cplx64 a, cplx64 b) {
+    const cplx64 r = cdiv(b, a);
+    G = cm(G, a);
+    if (is_one(r)) return;
+    SchedOp o{};
+    o.k = 1;
+    o.q[0] = (uint8_t)q;
+    o.mono = 1;
+    o.perm = 0;
+    o.urows = 1;
+    o.mat = put({{1.0, 0.0}, r});
+    o.dense = put({{1.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, r});
+    out.push_back(o);
+  }
+  void flush(int q) {
+    if (is_one(pa[q]) && is_one(pb[q])) return;
+    emit_phase(q, pa[q], pb[q]);
+    pa[q] = pb[q] = {1.0, 0.0};
+  }
+  void emit_scalar(int q) {
+    if (is_one(G)) return;
+    SchedOp o{};
+    o.k = 1;
+    o.q[0] = (uint8_t)q;
+    o.mono = 1;
+    o.perm = 0;
+    o.mat = put({G, G});
+    o.dense = put({G, {0.0, 0.0}, {0.0, 0.0}, G});
+    out.push_back(o);
+    G = {1.0, 0.0};
+  }
+  void emit_x(int q) {
+    SchedOp o{};
+    o.k = 1;
+    o.q[0] = (uint8_t)q;
+    o.mono = 1;
+    o.perm = 1;
+    o.unit = 1;
+    o.urows = 3;
+    o.mat = put({{1.0, 0.0}, {1.0, 0.0}});
+    o.dense = put({{0.0, 0.0}, {1.0, 0.0}, {1.0, 0.0}, {0.0, 0.0}});
+    out.push_back(o);
+  }
+  // real rotation [[c, -s], [s, c]] (c^2 + s^2 = 1), normalised by max(c, s)
+  void emit_rotation(int q, double c, double s) {
+    SchedOp o{};
+    o.k = 1;
+    o.q[0] = (uint8_t)q;
+    if (c >= s) {
+      const double t = s / c;
+      G = cm(G, {c, 0.0});
+      o.rot = 1;
+      o.dense = put({{1.0, 0.0}, {-t, 0.0}, {t, 0.0}, {1.0, 0.0}});
+    } else {
+      const double u = c / s;
+      G = cm(G, {s, 0.0});
+      o.rot = 2;
+      o.dense = put({{u, 0.0}, {-1.0, 0.0}, {1.0, 0.0}, {u, 0.0}});
+    }
+    o.mat = o.dense;
+    out.push_back(o);
+    // keep the scale of the intermediate state within 2^+-100
+    const double g2 = cabs2(G);
+    if (g2 < 0x1p-200 || g2 > 0x1p200) emit_scalar(q);
+  }
+  // dense one-qubit U (row-major) on q, after the pending diagonal of q
+  void dense1(const SchedOp& src) {
+    const int q = src.q[0];
+    const cplx64* U0 = pool.data() + src.dense;
+    const cplx64 A = cm(U0[0], pa[q]), B = cm(U0[1], pb[q]), C = cm(U0[2], pa[q]), D = cm(U0[3], pb[q]);
+    const double n0 = cabs2(A) + cabs2(C), n1 = cabs2(B) + cabs2(D);
+    const cplx64 ip{A.re * B.re + A.im * B.im + C.re * D.re + C.im * D.im,
+                    A.re * B.im - A.im * B.re + C.re * D.im - C.im * D.re};   // conj(A) B + conj(C) D
+    const bool unitary = std::fabs(n0 - 1.0) < 1e-12 && std::fabs(n1 - 1.0) < 1e-12 && cabs2(ip) < 1e-24;
+    const double c0 = std::sqrt(cabs2(A)), s0 = std::sqrt(cabs2(C));
+    if (unitary && s0 == 0.0 && cabs2(B) == 0.0) {     // diagonal: joins the pending diagonal
+      pa[q] = A;
+      pb[q] = D;
+      return;
+    }
+    if (unitary && c0 == 0.0 && cabs2(D) == 0.0) {     // anti-diagonal: X, then diag(B, C)
+      emit_x(q);
+      pa[q] = B;
+      pb[q] = C;
+      return;
+    }
+    if (unitary && c0 > 0.0 && s0 > 0.0) {
+      const double r = std::hypot(c0, s0);
+      const double c = c0 / r, s = s0 / r;
+      const cplx64 d0 = cdiv(A, {c, 0.0}), d1 = cdiv(C, {s, 0.0});
+      const cplx64 e1 = cdiv({-B.re, -B.im}, cm(d0, {s, 0.0}));
+      const cplx64 Dr = cm(cm(d1, {c, 0.0}), e1);           // the rebuilt entry D
+      if (cabs2({Dr.re - D.re, Dr.im - D.im}) < 1e-28) {
+        emit_phase(q, {1.0, 0.0}, e1);
+        emit_rotation(q, c, s);
+        pa[q] = d0;
+        pb[q] = d1;
+        return;
+      }
+    }
+    // not unitary (or not rebuilt exactly enough): dense, with the pending diagonal in its columns
+    SchedOp o = src;
+    o.dense = o.mat = put({A, B, C, D});
+    o.norm = 0;
+    o.rot = 0;
+    pa[q] = pb[q] = {1.0, 0.0};
+    out.push_back(o);
+  }
+  // two-qubit monomial: the pending diagonals pass through the permutation and
+  // factor per qubit; the non-factoring part is a phase on the |11> row
+  void mono2(const SchedOp& src) {
+    const int q0 = src.q[0], q1 = src.q[1];
+    cplx64 ph[4];
+    for (int r = 0; r < 4; ++r) ph[r] = src.unit ? cplx64{1.0, 0.0} : pool[src.mat + r];
+    cplx64 Dp[4];
+    for (int r = 0; r < 4; ++r) {
+      const int col = (src.perm >> (2 * r)) & 3;
+      const cplx64 dl = cm((col & 1) ? pb[q0] : pa[q0], (col & 2) ? pb[q1] : pa[q1]);
+      Dp[r] = cm(ph[r], dl);
+    }
+    const cplx64 s0 = Dp[0];
+    const cplx64 x1 = cdiv(Dp[1], s0), y1 = cdiv(Dp[2], s0);
+    const cplx64 gamma = cdiv(Dp[3], cm(s0, cm(x1, y1)));
+    G = cm(G, s0);
+    pa[q0] = pa[q1] = {1.0, 0.0};
+    pb[q0] = x1;
+    pb[q1] = y1;
+    SchedOp o = src;
+    const bool unit = is_one(gamma);
+    o.unit = unit ? 1 : 0;
+    o.urows = unit ? 15 : 7;
+    o.mat = put({{1.0, 0.0}, {1.0, 0.0}, {1.0, 0.0}, gamma});
+    o.dense = (uint32_t)pool.size();
+    for (int r = 0; r < 4; ++r)
+      for (int c = 0; c < 4; ++c) {
+        const bool hit = ((src.perm >> (2 * r)) & 3) == c;
+        pool.push_back(hit ? (r == 3 ? gamma : cplx64{1.0, 0.0}) : cplx64{0.0, 0.0});
+      }
+    out.push_back(o);
+  }
+  // dense k-qubit operation: the pending diagonals scale its columns
+  void dense_k(const SchedOp& src) {
+    const int d = 1 << src.k;
+    SchedOp o = src;
+    o.dense = o.mat = (uint32_t)pool.size();
+    for (int r = 0; r < d; ++r)
+      for (int c = 0; c < d; ++c) {
+        cplx64 f{1.0, 0.0};
+        for (int j = 0; j < src.k; ++j) f = cm(f, ((c >> j) & 1) ? pb[src.q[j]] : pa[src.q[j]]);
+        pool.push_back(cm(pool[src.dense + r * d + c], f));
+      }
+    for (int j = 0; j < src.k; ++j) pa[src.q[j]] = pb[src.q[j]] = {1.0, 0.0};
+    out.push_back(o);
+  }
+};
+
+}  // namespace
+
+void decompose_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& pool) {
+  std::vector<SchedOp> out;
+  out.reserve(ops.size() * 2);
+  Decomposer dc(out, pool);
+  int last_q = 0;
+  for (const SchedOp& o : ops) {
+    if (o.grad) {
+      for (int j = 0; j < o.k; ++j) dc.flush(o.q[j]);
+      out.push_back(o);
+    } else if (o.k == 1 && !o.mono) {
+      dc.dense1(o);
+    } else if (o.k == 1) {             // one-qubit monomial: diagonal, or X with phases
+      const int q = o.q[0];
+      const cplx64 p0 = o.unit ? cplx64{1.0, 0.0} : pool[o.mat], p1 = o.unit ? cplx64{1.0, 0.0} : pool[o.mat + 1];
+      if (o.perm & 1) {
+        dc.emit_x(q);
+        const cplx64 a = cm(p0, dc.pb[q]), b = cm(p1, dc.pa[q]);
+        dc.pa[q] = a;
+        dc.pb[q] = b;
+      } else {
+        dc.pa[q] = cm(dc.pa[q], p0);
+        dc.pb[q] = cm(dc.pb[q], p1);
+      }
+    } else if (o.k == 2 && o.mono) {
+      dc.mono2(o);
+    } else {
+      dc.dense_k(o);
+    }
+    last_q = o.q[0];
+  }
+  for (int q = 0; q < 64; ++q) dc.flush(q);
+  dc.emit_scalar(last_q);
+  ops.swap(out);
 }
 
 // ------------------------------------------------------------ adjoint builder

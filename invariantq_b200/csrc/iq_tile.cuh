@@ -81,6 +81,20 @@ __device__ __forceinline__ void n1r(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
+// normalised real rotation (OP_R1R): FORM 0 [[1, -t], [t, 1]] (t = Re m[2]),
+// FORM 1 [[u, -1], [1, u]] (u = Re m[0]); 2 FMAs per amplitude
+template <int R, int S, int FORM>
+__device__ __forceinline__ void r1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
+  const double w = FORM == 0 ? ld_mat(m, 2).x : ld_mat(m, 0).x;
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & (1 << S)) continue;
+    const double2 x = s[v], y = s[v | (1 << S)];
+    d[v] = rot_row0<FORM>(w, x, y);
+    d[v | (1 << S)] = rot_row1<FORM>(w, x, y);
+  }
+}
+
 template <int R, int S, bool SW, bool UNIT>
 __device__ __forceinline__ void m1r_t(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
   double2 p0 = make_double2(1.0, 0.0), p1 = p0;
@@ -361,6 +375,18 @@ __device__ __forceinline__ void disp_n1r(int sl, int col, const double2 (&s)[1 <
   }
 }
 template <int R, int S = 0>
+__device__ __forceinline__ void disp_r1r(int sl, int form, const double2 (&s)[1 << R], double2 (&d)[1 << R],
+                                         const double2* m) {
+  if constexpr (S < R) {
+    if (sl == S) {
+      if (form) r1r<R, S, 1>(s, d, m);
+      else r1r<R, S, 0>(s, d, m);
+    } else {
+      disp_r1r<R, S + 1>(sl, form, s, d, m);
+    }
+  }
+}
+template <int R, int S = 0>
 __device__ __forceinline__ void disp_m1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
                                          int perm, bool unit) {
   if constexpr (S < R) {
@@ -455,6 +481,7 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
     }
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
     case OP_N1R: disp_n1r<R>(od.a, od.perm, s, d, m); break;
+    case OP_R1R: disp_r1r<R>(od.a, od.perm, s, d, m); break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
     case OP_D2R:
       // one jump over the ordered slot pair (a, b) instead of nested compares

@@ -100,6 +100,7 @@ struct Emu {
         switch (od.kind) {
           case OP_D1R:
           case OP_N1R:   // stored whole (its unit entry included)
+          case OP_R1R:
             for (int L = 0; L < 8; ++L)
               for (int v = 0; v < NV; ++v) {
                 if (v & (1 << od.a)) continue;
@@ -387,7 +388,10 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
     std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(e.pool.data()),
                            reinterpret_cast<const cplx64*>(e.pool.data()) + e.pool.size());
     ops = fuse_two_qubit_blocks(ops, cp, fuse == 2);
-    if (fuse == 2) normalize_one_qubit_ops(ops, cp);
+    if (fuse == 2) {
+      decompose_one_qubit_ops(ops, cp);
+      normalize_one_qubit_ops(ops, cp);
+    }
     e.pool.assign(reinterpret_cast<const cd*>(cp.data()), reinterpret_cast<const cd*>(cp.data()) + cp.size());
   }
   SchedParams p{};
@@ -465,7 +469,10 @@ extern "C" int emu_jit_sources(int nbits, int M, int c, int R, int max_stages, d
   std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(pool.data()),
                          reinterpret_cast<const cplx64*>(pool.data()) + pool.size());
   if (fuse) ops = fuse_two_qubit_blocks(ops, cp, fuse == 2);
-  if (fuse == 2) normalize_one_qubit_ops(ops, cp);
+  if (fuse == 2) {
+    decompose_one_qubit_ops(ops, cp);
+    normalize_one_qubit_ops(ops, cp);
+  }
   SchedParams p{};
   p.nbits = nbits;
   p.M = M;

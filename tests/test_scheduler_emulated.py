@@ -144,7 +144,7 @@ def test_emulated_passes_match_oracle(port, emu, n, M, c, R, stages, budget, see
     # fuse 2: the specialised kernels' planning (CX/CZ/SWAP apart, normalised one-qubit gates)
     for fuse in (0, 1, 2):
         got, npasses, per = run_emu(emu, n, lsb, start, M=M, c=c, R=R, max_stages=stages, budget=budget, fuse=fuse)
-        assert per.sum() <= len(ops)
+        assert fuse == 2 or per.sum() <= len(ops)    # style 2 splits one-qubit gates into rotations and phases
         assert fuse or per.sum() == len(ops)
         assert np.max(np.abs(got - ref)) < 1e-12
 
