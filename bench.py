@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--nbuf", type=int, default=None)
     ap.add_argument("--reg-slots", type=int, default=None, help="register slots R of the tile kernel (3, 4, 5)")
     ap.add_argument("--ctas-per-sm", type=int, default=None, help="resident tile-pass CTAs per SM")
+    ap.add_argument("--jit-threads", type=int, default=None, help="CTA size of the specialised kernels")
     ap.add_argument("--jit", type=int, default=None, choices=[0, 1, 2],
                     help="specialised pass kernels: 0 off, 1 library default, 2 always")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -573,7 +574,7 @@ def our_arm(args, rank, world, local_rank):
     sv = NativeStateVector(n)
     for key, val in (("tile_bits", args.tile_bits), ("chunk_bits", args.chunk_bits), ("budget", args.budget),
                      ("max_stages", args.max_stages), ("nbuf", args.nbuf), ("reg_slots", args.reg_slots),
-                     ("ctas_per_sm", args.ctas_per_sm), ("jit", args.jit)):
+                     ("ctas_per_sm", args.ctas_per_sm), ("jit_threads", args.jit_threads), ("jit", args.jit)):
         if val is not None:
             sv.set_option(key, val)
     t_rec = time.perf_counter()

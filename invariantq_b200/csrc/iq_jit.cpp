@@ -252,22 +252,23 @@ bool get_cubin(const std::string& src, std::string& cubin, std::string& err) {
   return true;
 }
 
+// CTA size written in the generated source's first line
+int source_NT(const std::string& src) {
+  const size_t p = src.find("NT=");
+  return p == std::string::npos ? 128 : atoi(src.c_str() + p + 3);
+}
+
 // load a cubin into the current context's cache entry (caller holds no lock)
-bool install(int dev, const std::string& src, const std::string& cubin, int R, std::string& err) {
+bool install(int dev, const std::string& src, const std::string& cubin, std::string& err) {
   const Driver& dr = driver();
   auto k = std::make_unique<JitKernel>();
   if (dr.load(&k->mod, cubin.data()) != CUDA_SUCCESS) { err = "cuModuleLoadData failed"; return false; }
   if (dr.getfn(&k->fn, k->mod, "iq_jit_pass") != CUDA_SUCCESS) { err = "cuModuleGetFunction failed"; return false; }
-  k->nt = tile_pass_threads(R);
+  k->nt = source_NT(src);
   JitState& S = state();
   std::lock_guard<std::mutex> lk(S.mu);
   S.cache.emplace(std::make_pair(dev, src), std::move(k));   // keeps the first if two raced
   return true;
-}
-
-int source_R(const std::string& src) {
-  const size_t p = src.find(" R=");
-  return p == std::string::npos ? 4 : atoi(src.c_str() + p + 3);
 }
 
 void worker_loop() {
@@ -292,7 +293,7 @@ void worker_loop() {
         stopping = S.stop;
       }
       ok = !stopping && cudaSetDevice(task.first) == cudaSuccess && cudaFree(nullptr) == cudaSuccess &&
-           install(task.first, task.second, cubin, source_R(task.second), err);
+           install(task.first, task.second, cubin, err);
     }
     {
       std::lock_guard<std::mutex> lk(S.mu);
@@ -317,7 +318,7 @@ bool jit_ready(std::string& err, int& dev) {
 }  // namespace
 
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks) {
+                 int min_blocks, int threads) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   if (!jit_ready(err, dev)) return false;
@@ -329,7 +330,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      srcs[i] = jit_pass_source(*passes[i], e, min_blocks);
+      srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads);
       if (srcs[i].empty()) continue;
       auto it = S.cache.find({dev, srcs[i]});
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
@@ -349,7 +350,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     for (auto& t : th) t.join();
     for (size_t j = 0; j < todo.size(); ++j) {
       if (cubins[j].empty()) { err = errs[j]; return false; }
-      if (!install(dev, srcs[todo[j]], cubins[j], passes[todo[j]]->R, err)) return false;
+      if (!install(dev, srcs[todo[j]], cubins[j], err)) return false;
     }
   }
   std::lock_guard<std::mutex> lk(S.mu);
@@ -362,7 +363,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
 }
 
 void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
-                int min_blocks) {
+                int min_blocks, int threads) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   std::string err;
@@ -373,7 +374,7 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      std::string src = jit_pass_source(*passes[i], e, min_blocks);
+      std::string src = jit_pass_source(*passes[i], e, min_blocks, threads);
       if (src.empty()) continue;
       std::pair<int, std::string> key(dev, std::move(src));
       auto it = S.cache.find(key);

@@ -33,14 +33,15 @@ struct JitKernel;
 // compile fails.
 // min_blocks: resident CTAs per SM the kernels are compiled for (the launch's
 // TileLaunch::ctas_per_sm).
+// threads: CTA size of the kernels (128, 256; 0 = by register slots).
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks);
+                 int min_blocks, int threads);
 
 // Kernels already compiled for these passes (null where none); with
 // queue_missing, the missing ones are queued for compilation on background
 // threads, so a later plan with the same structure finds them.
 void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
-                int min_blocks);
+                int min_blocks, int threads);
 
 // Wait (at most timeout_s) until the background compilations have finished.
 bool jit_wait(double timeout_s);

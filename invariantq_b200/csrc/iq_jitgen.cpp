@@ -202,7 +202,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
 }  // namespace
 
 // Source of the kernel specialised to pass `d` (see iq_plan.h).
-std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks) {
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads) {
   if (d.ngrad || d.nsets > 1) {
     err = "adjoint passes are not specialised";
     return "";
@@ -211,12 +211,12 @@ std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks)
     err = "register slots out of range";
     return "";
   }
-  const int NT = tile_pass_threads(d.R);
+  const int NT = (threads == 128 || threads == 256) ? threads : tile_pass_threads(d.R);
   const int MINB = d.R == 5 ? 1 : (min_blocks >= 1 && min_blocks <= 4 ? min_blocks : 2);
   const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
   Gen g;
   std::ostringstream& o = g.o;
-  o << "// generated by iq_jitgen (iq-jit-1): M=" << (int)d.M << " c=" << (int)d.c << " R=" << (int)d.R
+  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " M=" << (int)d.M << " c=" << (int)d.c << " R=" << (int)d.R
     << " stages=" << (int)d.nstages << " ops=" << d.nops << "\n";
   o << "#include \"iq_pipe.cuh\"\nusing namespace iqb;\n";
   o << "struct JitMats { double2 m[" << nmat << "]; };\n";

@@ -214,6 +214,7 @@ struct Engine {
   static constexpr int kJitMinBits = 18;
   int normalize = 1;   // normalised one-qubit operations in specialised passes
   int plan_style = 0;  // 0: by the jit setting; 1: as for the interpreting kernel; 2: as for specialised kernels
+  int jit_threads = 0; // CTA size of specialised kernels (0: by register slots; 128 or 256)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
 
   double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0, st_h2d = 0;
@@ -406,12 +407,12 @@ struct Engine {
     for (auto& pl : pg.plans) ds.push_back(&pl.desc);
     if (own || jit >= 2) {
       std::string err;
-      if (!jit_prepare(ds, pg.jit, err, tl.ctas_per_sm)) {
+      if (!jit_prepare(ds, pg.jit, err, tl.ctas_per_sm, jit_threads)) {
         jit_note(err);
         pg.jit.clear();
       }
     } else {
-      jit_lookup(ds, pg.jit, true, tl.ctas_per_sm);
+      jit_lookup(ds, pg.jit, true, tl.ctas_per_sm, jit_threads);
     }
     bool any = false;
     for (auto* k : pg.jit) any |= k != nullptr;
@@ -1129,6 +1130,7 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   else if (!strcmp(key, "jit")) { if (iv < 0 || iv > 2) return -1; e->jit = iv; }
   else if (!strcmp(key, "normalize")) e->normalize = iv ? 1 : 0;
   else if (!strcmp(key, "plan_style")) { if (iv < 0 || iv > 2) return -1; e->plan_style = iv; }
+  else if (!strcmp(key, "jit_threads")) { if (iv != 0 && iv != 128 && iv != 256) return -1; e->jit_threads = iv; }
   else if (!strcmp(key, "inject_status")) {   // failure-path tests: as if a tile pass had timed out
     if (iv < 1 || iv > 2) return -1;
     if (!cuda_ok(cudaMemcpyAsync(e->d_status, &iv, sizeof(int), cudaMemcpyHostToDevice, e->stream), "inject status") ||
@@ -1157,6 +1159,7 @@ double iq_handle_get_option(void* h, const char* key) {
   if (!strcmp(key, "jit")) return e->jit;
   if (!strcmp(key, "normalize")) return e->normalize;
   if (!strcmp(key, "plan_style")) return e->plan_style;
+  if (!strcmp(key, "jit_threads")) return e->jit_threads;
   return kNaN;
 }
 
