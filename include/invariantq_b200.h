@@ -268,7 +268,8 @@ int iq_ansatz_energy(const iq_adjoint_circuit* circuit);
 /* Counters of the calling thread's last adjoint / energy call: out[0] jobs,
  * [1] forward passes, [2] backward passes, [3] kernel launches, [4] algorithmic
  * HBM bytes of the passes, [5] host preparation ms (summed over workers),
- * [6] wall ms, [7] streams used.  Returns the number of counters (8). */
+ * [6] wall ms, [7] streams used, [8] passes run by specialised kernels
+ * (IQ_ADJOINT_JIT, default 1).  Returns the number of counters (9). */
 int iq_adjoint_stats(double* out, size_t n);
 
 /* Failure-path check (no counterpart in the reference): one CTA waits, with

@@ -42,6 +42,7 @@
 
 #include "../../include/invariantq_b200.h"
 #include "iq_c64.h"
+#include "iq_jit.h"
 #include "iq_kernels.h"
 #include "iq_plan.h"
 
@@ -64,14 +65,15 @@ struct Cfg {
   SchedParams sp{};
   TileLaunch tl{};
   int fuse = 1;
+  int jit = 1;   // specialised kernels (iq_jit.cpp) for the forward and backward passes
   static Cfg from_env() {
     Cfg c;
+    c.jit = env_int("IQ_ADJOINT_JIT", 1);
     c.sp.M = env_int("IQ_TILE_BITS", 11);
     c.sp.c = env_int("IQ_CHUNK_BITS", 5);
     c.sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
-    // adjoint sweeps: a larger budget than the state-vector default (80) -- their
-    // passes are cheaper per operation (structured rotations, unit CZ phases)
+    // adjoint sweeps plan with the same budget as the state-vector default
     c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 120.0));
     c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
     c.tl.nbuf = env_int("IQ_NBUF", 3);
@@ -151,6 +153,7 @@ struct Shape {
   unsigned grid = 0;       // tile-pass grid (gradient partials row length)
   int ngrads = 0;
   std::vector<int> grad_param;
+  std::vector<const JitKernel*> jit;   // specialised kernel per pass (null: interpreting kernel)
 };
 
 bool same_op(const SchedOp& a, const SchedOp& b) {
@@ -212,6 +215,12 @@ bool make_shape(const Cfg& cfg, int nbits, const std::vector<SchedOp>& fused, si
       s.grid = g;
     }
   }
+  if (cfg.jit) {   // kernels specialised to the passes (shared by every circuit with the same pass structure)
+    std::vector<const PassDesc*> ds;
+    for (const PassPlan& pl : s.plans) ds.push_back(&pl.desc);
+    std::string jerr;
+    if (!jit_prepare(ds, s.jit, jerr, cfg.tl.ctas_per_sm, 0, true)) s.jit.clear();
+  }
   return true;
 }
 
@@ -256,7 +265,7 @@ int joint_bits(int n) { return std::max(n + 1, 7); }
 // ---------------------------------------------------------------- workspace
 
 struct Stats {
-  std::atomic<uint64_t> jobs{0}, fw_passes{0}, bw_passes{0}, launches{0}, replans{0};
+  std::atomic<uint64_t> jobs{0}, fw_passes{0}, bw_passes{0}, launches{0}, replans{0}, jit_passes{0};
   std::atomic<uint64_t> bytes{0};           // algorithmic HBM bytes of the passes
   std::atomic<uint64_t> host_ns{0};
 };
@@ -459,9 +468,15 @@ bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double
     d.set_mat_stride = mat_stride;
     d.grad_stride = grad_stride;
     if (grid) *grid = tile_pass_grid(d, cfg.tl, w.num_sms);
-    if (!cuda_ok(launch_tile_pass((*tm)[i], d, mats, w.status.p, cfg.tl, w.num_sms, w.stream, gpart),
-                 "tile pass kernel", err))
+    if (i < s.jit.size() && s.jit[i]) {
+      if (!cuda_ok(jit_launch_sets(s.jit[i], (*tm)[i], d, mats, w.status.p, cfg.tl, w.num_sms, w.stream, gpart),
+                   "specialised tile pass kernel", err))
+        return false;
+      ++st.jit_passes;
+    } else if (!cuda_ok(launch_tile_pass((*tm)[i], d, mats, w.status.p, cfg.tl, w.num_sms, w.stream, gpart),
+                        "tile pass kernel", err)) {
       return false;
+    }
   }
   st.launches += s.plans.size();
   st.bytes += (uint64_t)s.plans.size() * nsets * (32ULL << s.nbits);
@@ -695,7 +710,7 @@ int current_device(std::string& err) {
   return dev;
 }
 
-thread_local double t_stats[8] = {0};
+thread_local double t_stats[9] = {0};
 
 // Workspaces kept between calls (streams, events and buffers are costly to
 // create and allocation synchronises the device).  A workspace holding more
@@ -816,6 +831,7 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   t_stats[5] = (double)st.host_ns.load() * 1e-6;
   t_stats[6] = wall;
   t_stats[7] = (double)nw;
+  t_stats[8] = (double)st.jit_passes.load();
   (void)st.replans;
   if (!first_err.empty()) {
     record_error(first_err.find("scheduler") == 0 ? E_STATE : E_CUDA, first_err.c_str());
@@ -1145,8 +1161,8 @@ int iq_adjoint_release(void) {
 
 int iq_adjoint_stats(double* out, size_t n) {
   if (!out) return -1;
-  for (size_t i = 0; i < n && i < 8; ++i) out[i] = t_stats[i];
-  return 8;
+  for (size_t i = 0; i < n && i < 9; ++i) out[i] = t_stats[i];
+  return 9;
 }
 
 }  // extern "C"

@@ -190,6 +190,7 @@ struct JitKernel {
   CUmodule mod = nullptr;
   CUfunction fn = nullptr;
   int nt = 128;
+  bool sets = false;     // shared-memory matrices per parameter set (interpreting kernel's arguments)
   std::atomic<int> smem_limit_set{0};
 };
 
@@ -265,6 +266,7 @@ bool install(int dev, const std::string& src, const std::string& cubin, std::str
   if (dr.load(&k->mod, cubin.data()) != CUDA_SUCCESS) { err = "cuModuleLoadData failed"; return false; }
   if (dr.getfn(&k->fn, k->mod, "iq_jit_pass") != CUDA_SUCCESS) { err = "cuModuleGetFunction failed"; return false; }
   k->nt = source_NT(src);
+  k->sets = src.find(" sets=1 ") != std::string::npos;
   JitState& S = state();
   std::lock_guard<std::mutex> lk(S.mu);
   S.cache.emplace(std::make_pair(dev, src), std::move(k));   // keeps the first if two raced
@@ -318,7 +320,7 @@ bool jit_ready(std::string& err, int& dev) {
 }  // namespace
 
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks, int threads) {
+                 int min_blocks, int threads, bool set_mode) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   if (!jit_ready(err, dev)) return false;
@@ -330,7 +332,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads);
+      srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
       if (srcs[i].empty()) continue;
       auto it = S.cache.find({dev, srcs[i]});
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
@@ -363,7 +365,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
 }
 
 void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
-                int min_blocks, int threads) {
+                int min_blocks, int threads, bool set_mode) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   std::string err;
@@ -374,7 +376,7 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
       std::string e;
-      std::string src = jit_pass_source(*passes[i], e, min_blocks, threads);
+      std::string src = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
       if (src.empty()) continue;
       std::pair<int, std::string> key(dev, std::move(src));
       auto it = S.cache.find(key);
@@ -430,6 +432,30 @@ cudaError_t jit_launch(const JitKernel* kc, const CUtensorMap& tm, const PassDes
   const double2* mats = d.mat_elems ? host_mats : zero_mat;
   void* args[] = {const_cast<CUtensorMap*>(&tm), const_cast<PassDesc*>(&d), const_cast<double2*>(mats), &dev_status,
                   &nbuf};
+  const unsigned grid = tile_pass_grid(d, tl, num_sms);
+  const CUresult r = dr.launch(k->fn, grid, 1, 1, (unsigned)k->nt, 1, 1, (unsigned)smem, (CUstream)st, args, nullptr);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+cudaError_t jit_launch_sets(const JitKernel* kc, const CUtensorMap& tm, const PassDesc& d, const double2* dev_mats,
+                            int* dev_status, const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials) {
+  JitKernel* k = const_cast<JitKernel*>(kc);
+  if (!k->sets) return cudaErrorInvalidValue;
+  if (d.ngrad && !grad_partials) return cudaErrorInvalidValue;
+  const Driver& dr = driver();
+  int nbuf = tl.nbuf < 1 ? 1 : (tl.nbuf > kMaxBufJit ? kMaxBufJit : tl.nbuf);
+  const size_t smem = 1024 + (size_t)nbuf * ((size_t)16 << d.M) + (size_t)d.mat_elems * 16 +
+                      (size_t)d.ngrad * (k->nt / 8) * 8;
+  if (!k->smem_limit_set.load(std::memory_order_acquire)) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (dr.setattr(k->fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, optin - 1024) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+    k->smem_limit_set.store(1, std::memory_order_release);
+  }
+  void* args[] = {const_cast<CUtensorMap*>(&tm), const_cast<PassDesc*>(&d), &dev_mats, &dev_status, &nbuf,
+                  &grad_partials};
   const unsigned grid = tile_pass_grid(d, tl, num_sms);
   const CUresult r = dr.launch(k->fn, grid, 1, 1, (unsigned)k->nt, 1, 1, (unsigned)smem, (CUstream)st, args, nullptr);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;

@@ -34,14 +34,16 @@ struct JitKernel;
 // min_blocks: resident CTAs per SM the kernels are compiled for (the launch's
 // TileLaunch::ctas_per_sm).
 // threads: CTA size of the kernels (128, 256; 0 = by register slots).
+// set_mode: the shared-memory form (passes over parameter sets, adjoint steps;
+// launched with jit_launch_sets).
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks, int threads);
+                 int min_blocks, int threads, bool set_mode = false);
 
 // Kernels already compiled for these passes (null where none); with
 // queue_missing, the missing ones are queued for compilation on background
 // threads, so a later plan with the same structure finds them.
 void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, bool queue_missing,
-                int min_blocks, int threads);
+                int min_blocks, int threads, bool set_mode = false);
 
 // Wait (at most timeout_s) until the background compilations have finished.
 bool jit_wait(double timeout_s);
@@ -50,6 +52,12 @@ bool jit_wait(double timeout_s);
 // (d.mat_elems complex values), copied into the launch's parameters.
 cudaError_t jit_launch(const JitKernel* k, const CUtensorMap& tm, const PassDesc& d, const double2* host_mats,
                        int* dev_status, const TileLaunch& tl, int num_sms, cudaStream_t st);
+
+// Launch a specialised pass of the shared-memory form with the interpreting
+// kernel's arguments (device matrix pool, gradient partials).
+cudaError_t jit_launch_sets(const JitKernel* k, const CUtensorMap& tm, const PassDesc& d, const double2* dev_mats,
+                            int* dev_status, const TileLaunch& tl, int num_sms, cudaStream_t st,
+                            double* grad_partials);
 
 // Kernels compiled and cubins loaded from the cache directory so far.
 void jit_counters(uint64_t* compiled, uint64_t* loaded_from_disk);

@@ -17,7 +17,10 @@ struct Gen {
   std::string fresh() { return "t" + std::to_string(tmp++); }
 };
 
-std::string mat(uint32_t i) { return "Mt.m[" + std::to_string(i) + "]"; }
+// matrix entry i of the pass's block: a kernel parameter, or (kernels for
+// several parameter sets) the current set's block in shared memory
+thread_local bool g_set_mode = false;
+std::string mat(uint32_t i) { return (g_set_mode ? "smat[" : "Mt.m[") + std::to_string(i) + "]"; }
 
 // Straight-line code of one stage.  cur[v] names the value register v of the
 // thread holds (v's bit i = register slot i).  Every operation is written with
@@ -189,6 +192,32 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         cur = out;
         break;
       }
+      case OP_GRAD2: {   // adjoint step: select bit in slot 0, qubit in slot b (shared-memory matrices only)
+        if (!g_set_mode) { err = "adjoint steps need the shared-memory form"; return false; }
+        const int B = 1 << od.b;
+        const std::string G = std::to_string((int)od.perm);
+        const std::string acc = g.fresh(), u0 = g.fresh(), u1 = g.fresh(), u3 = g.fresh();
+        o << "        const double2 " << u0 << " = " << mat(m + 0) << ", " << u1 << " = " << mat(m + 1) << ", " << u3
+          << " = " << mat(m + 3) << ";\n";
+        o << "        double " << acc << " = 0.0;\n";
+        for (int v = 0; v < NV; ++v) {
+          if (v & (1 | B)) continue;
+          const std::string p0 = cur[v], p1 = cur[v | B], l0 = cur[v | 1], l1 = cur[v | 1 | B];
+          o << "        " << acc << " += grad_term<" << G << ">(" << p0 << ", " << p1 << ", " << l0 << ", " << l1 << ");\n";
+          const std::string a = g.fresh(), b = g.fresh(), c = g.fresh(), d2 = g.fresh();
+          o << "        double2 " << a << ", " << b << ", " << c << ", " << d2 << ";\n";
+          o << "        unrotate<" << G << ">(" << p0 << ", " << p1 << ", " << a << ", " << b << ", " << u0 << ", " << u1 << ", "
+            << u3 << ");\n";
+          o << "        unrotate<" << G << ">(" << l0 << ", " << l1 << ", " << c << ", " << d2 << ", " << u0 << ", " << u1
+            << ", " << u3 << ");\n";
+          cur[v] = a;
+          cur[v | B] = b;
+          cur[v | 1] = c;
+          cur[v | 1 | B] = d2;
+        }
+        o << "        grad_accumulate(" << acc << ", gs + " << od.gidx << ", lane8, omask);\n";
+        break;
+      }
       default:
         err = "operation kind " + std::to_string((int)od.kind) + " is not specialised";
         return false;
@@ -202,11 +231,12 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
 }  // namespace
 
 // Source of the kernel specialised to pass `d` (see iq_plan.h).
-std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads) {
-  if (d.ngrad || d.nsets > 1) {
-    err = "adjoint passes are not specialised";
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads, bool set_mode) {
+  if (!set_mode && (d.ngrad || d.nsets > 1)) {
+    err = "passes over several parameter sets need the shared-memory form";
     return "";
   }
+  g_set_mode = set_mode;
   if (d.R < 3 || d.R > kMaxK) {
     err = "register slots out of range";
     return "";
@@ -216,9 +246,28 @@ std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks,
   const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
   Gen g;
   std::ostringstream& o = g.o;
-  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " M=" << (int)d.M << " c=" << (int)d.c << " R=" << (int)d.R
+  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " sets=" << (set_mode ? 1 : 0) << " M=" << (int)d.M
+    << " c=" << (int)d.c << " R=" << (int)d.R
     << " stages=" << (int)d.nstages << " ops=" << d.nops << "\n";
   o << "#include \"iq_pipe.cuh\"\nusing namespace iqb;\n";
+  if (set_mode) {
+    o << "struct JitStages {\n  int lane8, octet;\n  unsigned omask;\n";
+    o << "  __device__ __forceinline__ void operator()(double2* tile, const double2* smat, double* gslots, bool work) {\n";
+    o << "    if (!work) return;\n";
+    o << "    double* const gs = gslots + octet * " << d.ngrad << ";\n    (void)gs;\n";
+    for (int s = 0; s < d.nstages; ++s)
+      if (!gen_stage(g, d, s, NT, err)) return "";
+    o << "  }\n};\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << MINB << ")\n"
+      << "iq_jit_pass(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,\n"
+      << "            const double2* __restrict__ mats, int* __restrict__ status, int nbuf,\n"
+      << "            double* __restrict__ grad_partials) {\n"
+      << "  extern __shared__ __align__(1024) unsigned char smem_raw[];\n"
+      << "  const int ctid = threadIdx.x;\n"
+      << "  JitStages st{ctid & 7, ctid >> 3, 0xFFu << (ctid & 24)};\n"
+      << "  set_tile_pass<" << NT << ">(tm, P, mats, status, nbuf, grad_partials, smem_raw, st);\n}\n";
+    return o.str();
+  }
   o << "struct JitMats { double2 m[" << nmat << "]; };\n";
   o << "struct JitBody {\n  const JitMats& Mt;\n  int lane8, octet;\n  unsigned omask;\n";
   o << "  __device__ __forceinline__ void operator()(double2* tile, unsigned long long, bool work) {\n";

@@ -157,6 +157,56 @@ __device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
   return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
 }
 
+// Adjoint step on slot 0 (psi / lambda select bit) and slot B (the qubit):
+// returns this thread's share of Im<lambda| P |psi> for generator P (GEN 0 = X,
+// 1 = Y, 2 = Z), then un-applies the rotation exp(-i t P / 2) on the qubit in
+// both halves.  m is the inverse rotation, used through its structure:
+// GEN 0: [[c, i s], [i s, c]]; GEN 1: [[c, s], [-s, c]] (real);
+// GEN 2: diag(e^{i t/2}, e^{-i t/2}).  Inputs are read before outputs are
+// written (in-place safe).
+template <int GEN>
+__device__ __forceinline__ void unrotate(double2 x0, double2 x1, double2& y0, double2& y1, double2 u0, double2 u1,
+                                         double2 u3) {
+  if (GEN == 0) {         // y0 = c x0 + i s x1, y1 = i s x0 + c x1
+    const double c = u0.x, sn = u1.y;
+    y0 = make_double2(fma(c, x0.x, -sn * x1.y), fma(c, x0.y, sn * x1.x));
+    y1 = make_double2(fma(c, x1.x, -sn * x0.y), fma(c, x1.y, sn * x0.x));
+  } else if (GEN == 1) {  // y0 = c x0 + s x1, y1 = c x1 - s x0
+    const double c = u0.x, sn = u1.x;
+    y0 = make_double2(fma(c, x0.x, sn * x1.x), fma(c, x0.y, sn * x1.y));
+    y1 = make_double2(fma(c, x1.x, -sn * x0.x), fma(c, x1.y, -sn * x0.y));
+  } else {                // diagonal phases
+    y0 = cmul(u0, x0);
+    y1 = cmul(u3, x1);
+  }
+}
+
+
+// this amplitude pair's share of Im <lambda| P |psi> for the generator P of an
+// adjoint step (GEN 0 = X, 1 = Y, 2 = Z); explicit FMA forms, so every kernel
+// rounds it the same way
+template <int GEN>
+__device__ __forceinline__ double grad_term(double2 p0, double2 p1, double2 l0, double2 l1) {
+  if (GEN == 0) {         // X: (P psi)_0 = psi_1, (P psi)_1 = psi_0
+    return fma(l0.x, p1.y, -(l0.y * p1.x)) + fma(l1.x, p0.y, -(l1.y * p0.x));
+  } else if (GEN == 1) {  // Y: (P psi)_0 = -i psi_1, (P psi)_1 = i psi_0
+    return fma(l1.x, p0.x, l1.y * p0.y) - fma(l0.x, p1.x, l0.y * p1.y);
+  } else {                // Z: (P psi)_0 = psi_0, (P psi)_1 = -psi_1
+    return fma(l0.x, p0.y, -(l0.y * p0.x)) - fma(l1.x, p1.y, -(l1.y * p1.x));
+  }
+}
+
+// the octet's eight lanes hold the same registers of eight tile rows: sum
+// their shares, and the octet's lane 0 -- the only writer of its row of
+// accumulators -- adds it there.  Tiles reach a CTA, and tile rows reach an
+// octet, in a fixed order, so the sums are reproducible bit for bit.
+__device__ __forceinline__ void grad_accumulate(double acc, double* slot, int lane8, unsigned omask) {
+  acc += __shfl_xor_sync(omask, acc, 1, 8);
+  acc += __shfl_xor_sync(omask, acc, 2, 8);
+  acc += __shfl_xor_sync(omask, acc, 4, 8);
+  if (lane8 == 0) *slot += acc;
+}
+
 constexpr int kMaxBuf = 4;
 
 template <int N>
@@ -284,9 +334,82 @@ __device__ __forceinline__ void tile_pipeline(const CUtensorMap& tm, const PassD
   bulk_wait_all();
 }
 
+// A pass over nsets arrays laid end to end (one per parameter set), each with
+// its own matrix block and gradient terms (PassDesc::nsets, set_shift,
+// set_mat_stride, grad_stride).  Dynamic shared memory: [tile buffers]
+// [the current set's matrix block][gradient accumulators: one row of ngrad per
+// octet of threads].  At a set boundary the CTA flushes the finished set's
+// gradient sums (octet rows summed in order, one column per CTA of
+// grad_partials) and loads the next set's matrices.  stages(buf, smat, gslots,
+// work) runs the pass's stages on a resident tile, each followed by a
+// __syncthreads() (or none at all when work is false: it is uniform in the CTA).
+template <int NT, class Stages>
+struct SetTileBody {
+  const PassDesc& P;
+  const double2* mats;
+  double* grad_partials;
+  double2* smat;
+  double* gslots;
+  uint32_t sshift;
+  uint32_t cur_set;
+  Stages& stages;
+
+  __device__ __forceinline__ void flush_grads() {
+    for (uint32_t i = threadIdx.x; i < P.ngrad; i += NT) {
+      double v = 0.0;
+      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
+      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_term[i]) * gridDim.x + blockIdx.x] = v;
+    }
+  }
+  __device__ __forceinline__ void operator()(double2* buf, unsigned long long t, bool work) {
+    const int tid = threadIdx.x;
+    const uint32_t tset = (uint32_t)(t >> sshift);   // uniform in the CTA
+    if (tset != cur_set) {   // every thread is past the previous tile's stages
+      if (P.ngrad) {
+        flush_grads();
+        __syncthreads();
+        for (uint32_t j = tid; j < P.ngrad * (NT / 8); j += NT) gslots[j] = 0.0;
+      }
+      cur_set = tset;
+      for (uint32_t j = tid; j < P.mat_elems; j += NT)
+        smat[j] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + j];
+      __syncthreads();
+    }
+    stages(buf, smat, gslots, work);
+  }
+};
+
+template <int NT, class Stages>
+__device__ __forceinline__ void set_tile_pass(const CUtensorMap& tm, const PassDesc& P, const double2* mats,
+                                              int* status, int nbuf, double* grad_partials, unsigned char* smem_raw,
+                                              Stages& stages);
+
 // 1024-byte aligned start of the dynamic shared memory (the tile buffers)
 __device__ __forceinline__ double2* aligned_tiles(unsigned char* smem_raw) {
   return reinterpret_cast<double2*>((reinterpret_cast<unsigned long long>(smem_raw) + 1023ull) & ~1023ull);
+}
+
+template <int NT, class Stages>
+__device__ __forceinline__ void set_tile_pass(const CUtensorMap& tm, const PassDesc& P, const double2* mats,
+                                              int* status, int nbuf, double* grad_partials, unsigned char* smem_raw,
+                                              Stages& stages) {
+  double2* tiles = aligned_tiles(smem_raw);
+  const int tid = threadIdx.x;
+  double2* smat = tiles + (size_t)nbuf * (1u << P.M);
+  const unsigned long long first = blockIdx.x;
+  // set of the tiles being processed (the CTA's tiles ascend, so each set is
+  // met in one run); its matrices sit in smat, its gradient sums in gslots
+  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
+  const uint32_t set0 = (first < P.ntiles) ? (uint32_t)(first >> sshift) : 0u;
+  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)set0 * P.set_mat_stride + i];
+  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
+  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
+  SetTileBody<NT, Stages> body{P, mats, grad_partials, smat, gslots, sshift, set0, stages};
+  tile_pipeline<NT>(tm, P, tiles, status, nbuf, body);
+  if (P.ngrad) {   // the last set's gradient partials
+    __syncthreads();
+    body.flush_grads();
+  }
 }
 
 }  // namespace iqb

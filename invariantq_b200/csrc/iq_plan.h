@@ -312,7 +312,12 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 // min_blocks: resident CTAs per SM the kernel's register budget is sized for
 // (launch bounds; 2 when out of 1..4; always 1 for R = 5); threads: CTA size
 // (128 or 256; otherwise tile_pass_threads(R)).
-std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2, int threads = 0);
+// set_mode: the form for passes over several parameter sets and adjoint steps
+// (matrices staged per set in shared memory, gradient accumulators; the
+// interpreting kernel's launch arguments); otherwise matrices are a kernel
+// parameter block.
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2, int threads = 0,
+                            bool set_mode = false);
 struct cplx64 { double re, im; };
 // Fuse runs of queued operations on at most two qubits into single 4x4 blocks
 // (a two-qubit operation absorbs the open one-qubit blocks of its qubits and

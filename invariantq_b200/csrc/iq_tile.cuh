@@ -308,30 +308,6 @@ __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
-// Adjoint step on slot 0 (psi / lambda select bit) and slot B (the qubit):
-// returns this thread's share of Im<lambda| P |psi> for generator P (GEN 0 = X,
-// 1 = Y, 2 = Z), then un-applies the rotation exp(-i t P / 2) on the qubit in
-// both halves.  m is the inverse rotation, used through its structure:
-// GEN 0: [[c, i s], [i s, c]]; GEN 1: [[c, s], [-s, c]] (real);
-// GEN 2: diag(e^{i t/2}, e^{-i t/2}).  Inputs are read before outputs are
-// written (in-place safe).
-template <int GEN>
-__device__ __forceinline__ void unrotate(double2 x0, double2 x1, double2& y0, double2& y1, double2 u0, double2 u1,
-                                         double2 u3) {
-  if (GEN == 0) {         // y0 = c x0 + i s x1, y1 = i s x0 + c x1
-    const double c = u0.x, sn = u1.y;
-    y0 = make_double2(fma(c, x0.x, -sn * x1.y), fma(c, x0.y, sn * x1.x));
-    y1 = make_double2(fma(c, x1.x, -sn * x0.y), fma(c, x1.y, sn * x0.x));
-  } else if (GEN == 1) {  // y0 = c x0 + s x1, y1 = c x1 - s x0
-    const double c = u0.x, sn = u1.x;
-    y0 = make_double2(fma(c, x0.x, sn * x1.x), fma(c, x0.y, sn * x1.y));
-    y1 = make_double2(fma(c, x1.x, -sn * x0.x), fma(c, x1.y, -sn * x0.y));
-  } else {                // diagonal phases
-    y0 = cmul(u0, x0);
-    y1 = cmul(u3, x1);
-  }
-}
-
 template <int R, int B, int GEN>
 __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
   const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u3 = ld_mat(m, 3);
@@ -340,13 +316,7 @@ __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)
   for (int v = 0; v < (1 << R); ++v) {
     if (v & (1 | (1 << B))) continue;
     const double2 p0 = s[v], p1 = s[v | (1 << B)], l0 = s[v | 1], l1 = s[v | 1 | (1 << B)];
-    if (GEN == 0) {         // X: (P psi)_0 = psi_1, (P psi)_1 = psi_0
-      acc += (l0.x * p1.y - l0.y * p1.x) + (l1.x * p0.y - l1.y * p0.x);
-    } else if (GEN == 1) {  // Y: (P psi)_0 = -i psi_1, (P psi)_1 = i psi_0
-      acc += (l1.x * p0.x + l1.y * p0.y) - (l0.x * p1.x + l0.y * p1.y);
-    } else {                // Z: (P psi)_0 = psi_0, (P psi)_1 = -psi_1
-      acc += (l0.x * p0.y - l0.y * p0.x) - (l1.x * p1.y - l1.y * p1.x);
-    }
+    acc += grad_term<GEN>(p0, p1, l0, l1);
     unrotate<GEN>(p0, p1, d[v], d[v | (1 << B)], u0, u1, u3);
     unrotate<GEN>(l0, l1, d[v | 1], d[v | 1 | (1 << B)], u0, u1, u3);
   }
@@ -447,17 +417,6 @@ __device__ __forceinline__ double disp_grad2_b(int sb, const double2 (&s)[1 << R
     return disp_grad2_b<R, GEN, B + 1>(sb, s, d, m);
   }
   return 0.0;
-}
-
-// the octet's eight lanes hold the same registers of eight tile rows: sum
-// their shares, and the octet's lane 0 -- the only writer of its row of
-// accumulators -- adds it there.  Tiles reach a CTA, and tile rows reach an
-// octet, in a fixed order, so the sums are reproducible bit for bit.
-__device__ __forceinline__ void grad_accumulate(double acc, double* slot, int lane8, unsigned omask) {
-  acc += __shfl_xor_sync(omask, acc, 1, 8);
-  acc += __shfl_xor_sync(omask, acc, 2, 8);
-  acc += __shfl_xor_sync(omask, acc, 4, 8);
-  if (lane8 == 0) *slot += acc;
 }
 
 // Apply one operation from s to d; returns true when it wrote the tile itself.
@@ -577,76 +536,28 @@ __device__ __forceinline__ void run_stage(double2* tile, const PassDesc& P, int 
   }
 }
 
-// Per-tile work of the interpreting kernel: switch the parameter set's
-// matrices (and flush its gradient sums) at set boundaries, then run the
-// pass's stages.
+// The interpreting kernel's stages: run_stage over the pass descriptor.
 template <int R, int NT>
-struct InterpBody {
+struct InterpStages {
   const PassDesc& P;
-  const double2* mats;
-  double* grad_partials;
-  double2* smat;
-  double* gslots;
-  uint32_t sshift;
-  uint32_t cur_set;
-
-  // gradient partials of the current set: octet rows summed in order, one
-  // column per CTA; rows the CTA never touches stay as the host zeroed them
-  __device__ __forceinline__ void flush_grads() {
-    for (uint32_t i = threadIdx.x; i < P.ngrad; i += NT) {
-      double v = 0.0;
-      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
-      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_term[i]) * gridDim.x + blockIdx.x] = v;
-    }
-  }
-  __device__ __forceinline__ void operator()(double2* buf, uint64_t t, bool work) {
-    const int tid = threadIdx.x;
-    const uint32_t tset = (uint32_t)(t >> sshift);   // uniform in the CTA
-    if (tset != cur_set) {   // every thread is past the previous tile's stages
-      if (P.ngrad) {
-        flush_grads();
-        __syncthreads();
-        for (uint32_t j = tid; j < P.ngrad * (NT / 8); j += NT) gslots[j] = 0.0;
-      }
-      cur_set = tset;
-      for (uint32_t j = tid; j < P.mat_elems; j += NT)
-        smat[j] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + j];
-      __syncthreads();
-    }
+  __device__ __forceinline__ void operator()(double2* buf, const double2* smat, double* gslots, bool work) {
     for (int s = 0; s < P.nstages; ++s) {
-      if (work) run_stage<R>(buf, P, s, smat, tid, NT, gslots);
+      if (work) run_stage<R>(buf, P, s, smat, threadIdx.x, NT, gslots);
       __syncthreads();
     }
   }
 };
 
-// The interpreting tile-pass kernel: NT threads per CTA run the pass's
-// stages (run_stage) on each tile the pipeline makes resident.
+// The interpreting tile-pass kernel: NT threads per CTA run the pass's stages
+// (run_stage) on each tile the pipeline makes resident.
 template <int R, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     tile_pass_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ PassDesc P,
                      const double2* __restrict__ mats, int* __restrict__ status, int nbuf,
                      double* __restrict__ grad_partials) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // [tile buffers, 1024-aligned for the 128-byte swizzle][pass matrix block]
-  // [gradient accumulators: one row of ngrad per octet of threads (adjoint passes)]
-  double2* tiles = aligned_tiles(smem_raw);
-  const int tid = threadIdx.x;
-  double2* smat = tiles + (size_t)nbuf * (1u << P.M);
-  const uint64_t first = blockIdx.x;
-  // set of the tiles being processed (the CTA's tiles ascend, so each set is
-  // met in one run); its matrices sit in smat, its gradient sums in gslots
-  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
-  const uint32_t set0 = (first < P.ntiles) ? (uint32_t)(first >> sshift) : 0u;
-  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)set0 * P.set_mat_stride + i];
-  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
-  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
-  InterpBody<R, NT> body{P, mats, grad_partials, smat, gslots, sshift, set0};
-  tile_pipeline<NT>(tm, P, tiles, status, nbuf, body);
-  if (P.ngrad) {   // the last set's gradient partials
-    __syncthreads();
-    body.flush_grads();
-  }
+  InterpStages<R, NT> stages{P};
+  set_tile_pass<NT>(tm, P, mats, status, nbuf, grad_partials, smem_raw, stages);
 }
 
 }  // namespace iqb

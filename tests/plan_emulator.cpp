@@ -504,3 +504,58 @@ extern "C" int emu_jit_sources(int nbits, int M, int c, int R, int max_stages, d
   memcpy(out, all.c_str(), all.size() + 1);
   return (int)plans.size();
 }
+
+// Sources of the kernels specialised to an ansatz's forward and backward
+// passes (shared-memory matrices, gradient accumulators: the adjoint
+// executor's form), planned as the executor plans them; separated by lines
+// "//@@PASS@@".  Returns the number of passes, or -1 (message in `out`).
+extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
+                                   const double* params, int M, int c, int R, int max_stages, double budget,
+                                   char* out, long long outlen) {
+  std::vector<AnsatzOp> ops(nops);
+  for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
+  std::string err, all;
+  if (ansatz_check(n, ops, err) < 0) {
+    snprintf(out, (size_t)outlen, "%s", err.c_str());
+    return -1;
+  }
+  int count = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<SchedOp> raw;
+    std::vector<cplx64> pool;
+    std::vector<int> gp;
+    if (pass == 0) ansatz_forward(n, ops, params, raw, pool);
+    else ansatz_backward(n, ops, params, raw, pool, gp);
+    const std::vector<SchedOp> fused = fuse_two_qubit_blocks(raw, pool);
+    SchedParams p{};
+    p.nbits = pass == 0 ? n : n + 1;
+    if (p.nbits < 7) continue;
+    p.M = M;
+    p.c = c;
+    p.R = R;
+    p.max_stages = max_stages;
+    p.budget = budget;
+    std::vector<PassPlan> plans;
+    if (plan_passes(p, fused, plans, err) < 0) {
+      snprintf(out, (size_t)outlen, "plan: %s", err.c_str());
+      return -1;
+    }
+    std::vector<cplx64> packed;
+    pack_pass_matrices(plans, pool.data(), packed);
+    for (const PassPlan& pl : plans) {
+      const std::string s = jit_pass_source(pl.desc, err, 2, 0, true);
+      if (s.empty()) {
+        snprintf(out, (size_t)outlen, "%s", err.c_str());
+        return -1;
+      }
+      if (count++) all += "\n//@@PASS@@\n";
+      all += s;
+    }
+  }
+  if ((long long)all.size() + 1 > outlen) {
+    snprintf(out, (size_t)outlen, "output buffer too small (%zu bytes needed)", all.size() + 1);
+    return -1;
+  }
+  memcpy(out, all.c_str(), all.size() + 1);
+  return count;
+}

@@ -158,3 +158,25 @@ def test_invalid_inputs_raise(G):
         G.adjoint_gradient(G.Ansatz(3, [("rx", (5,), 0)]), G.PauliHamiltonian.tfim(3), np.zeros(1))
     e, g = G.adjoint_gradient(a, G.PauliHamiltonian(3, [0.5], ["IIZ"]), np.array([0.3]))
     assert abs(e - 0.5) < 1e-15 and abs(g[0]) < 1e-15
+
+
+def test_specialised_kernels_equal_interpreting(G, monkeypatch):
+    """IQ_ADJOINT_JIT = 1 (kernels generated per pass structure, default) and 0
+    (interpreting kernel) run the same plans with the same arithmetic:
+    energies and gradients are identical, for one set and for sets batched
+    in one launch (adjoint steps, set switches, gradient accumulators)."""
+    rng = np.random.default_rng(31)
+    jobs = []
+    for n, L in [(12, 3), (9, 2)]:
+        a, h = G.Ansatz.hardware_efficient(n, L), G.PauliHamiltonian.tfim(n, 0.8)
+        jobs.append((a, h, rng.uniform(0, 2 * np.pi, (4, a.num_params))))
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("IQ_ADJOINT_JIT", flag)
+        out[flag] = G.adjoint_gradient_batch(jobs, num_streams=2)
+        st = G.adjoint_stats()
+        assert (st["specialised_passes"] > 0) == (flag == "1")
+        out[flag + "s"] = G.adjoint_gradient(jobs[0][0], jobs[0][1], jobs[0][2][1])
+    for (e0, g0), (e1, g1) in zip(out["0"], out["1"]):
+        assert np.array_equal(e0, e1) and np.array_equal(g0, g1)
+    assert out["0s"][0] == out["1s"][0] and np.array_equal(out["0s"][1], out["1s"][1])
