@@ -204,9 +204,11 @@ namespace {
 struct JitState {
   std::mutex mu;
   std::condition_variable cv, idle;
+  // keyed by (device, jit_pass_key); queued tasks carry the source to compile
   std::map<std::pair<int, std::string>, std::unique_ptr<JitKernel>> cache;
   std::set<std::pair<int, std::string>> pending;
-  std::deque<std::pair<int, std::string>> queue;
+  struct Task { int dev; std::string key, src; };
+  std::deque<Task> queue;
   std::vector<std::thread> workers;
   int busy = 0;
   bool stop = false;
@@ -222,7 +224,7 @@ void drain_at_exit() {
   JitState& S = state();
   std::unique_lock<std::mutex> lk(S.mu);
   S.stop = true;
-  for (auto& k : S.queue) S.pending.erase(k);
+  for (auto& t : S.queue) S.pending.erase({t.dev, t.key});
   S.queue.clear();
   S.idle.wait_for(lk, std::chrono::seconds(60), [&] { return S.busy == 0; });
 }
@@ -260,7 +262,7 @@ int source_NT(const std::string& src) {
 }
 
 // load a cubin into the current context's cache entry (caller holds no lock)
-bool install(int dev, const std::string& src, const std::string& cubin, std::string& err) {
+bool install(int dev, const std::string& key, const std::string& src, const std::string& cubin, std::string& err) {
   const Driver& dr = driver();
   auto k = std::make_unique<JitKernel>();
   if (dr.load(&k->mod, cubin.data()) != CUDA_SUCCESS) { err = "cuModuleLoadData failed"; return false; }
@@ -269,14 +271,14 @@ bool install(int dev, const std::string& src, const std::string& cubin, std::str
   k->sets = src.find(" sets=1 ") != std::string::npos;
   JitState& S = state();
   std::lock_guard<std::mutex> lk(S.mu);
-  S.cache.emplace(std::make_pair(dev, src), std::move(k));   // keeps the first if two raced
+  S.cache.emplace(std::make_pair(dev, key), std::move(k));   // keeps the first if two raced
   return true;
 }
 
 void worker_loop() {
   JitState& S = state();
   for (;;) {
-    std::pair<int, std::string> task;
+    JitState::Task task;
     {
       std::unique_lock<std::mutex> lk(S.mu);
       // after stop (process exit) the worker stays parked here: returning would
@@ -287,20 +289,20 @@ void worker_loop() {
       ++S.busy;
     }
     std::string cubin, err;
-    bool ok = get_cubin(task.second, cubin, err);
+    bool ok = get_cubin(task.src, cubin, err);
     if (ok) {
       bool stopping;
       {
         std::lock_guard<std::mutex> lk(S.mu);
         stopping = S.stop;
       }
-      ok = !stopping && cudaSetDevice(task.first) == cudaSuccess && cudaFree(nullptr) == cudaSuccess &&
-           install(task.first, task.second, cubin, err);
+      ok = !stopping && cudaSetDevice(task.dev) == cudaSuccess && cudaFree(nullptr) == cudaSuccess &&
+           install(task.dev, task.key, task.src, cubin, err);
     }
     {
       std::lock_guard<std::mutex> lk(S.mu);
       if (!ok && !err.empty()) S.last_error = err;
-      S.pending.erase(task);
+      S.pending.erase({task.dev, task.key});
       --S.busy;
     }
     S.idle.notify_all();
@@ -325,18 +327,19 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
   int dev = 0;
   if (!jit_ready(err, dev)) return false;
   JitState& S = state();
-  std::vector<std::string> srcs(passes.size());
-  std::vector<int> todo;                      // first pass of each source not yet cached
+  std::vector<std::string> keys(passes.size()), srcs(passes.size());
+  std::vector<int> todo;                      // first pass of each structure not yet cached
   {
     std::set<std::string> seen;
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
+      keys[i] = jit_pass_key(*passes[i], min_blocks, threads, set_mode);
+      auto it = S.cache.find({dev, keys[i]});
+      if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
+      if (!seen.insert(keys[i]).second) continue;
       std::string e;
       srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
-      if (srcs[i].empty()) continue;
-      auto it = S.cache.find({dev, srcs[i]});
-      if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
-      if (seen.insert(srcs[i]).second) todo.push_back((int)i);
+      if (!srcs[i].empty()) todo.push_back((int)i);
     }
   }
   if (!todo.empty()) {
@@ -352,13 +355,13 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     for (auto& t : th) t.join();
     for (size_t j = 0; j < todo.size(); ++j) {
       if (cubins[j].empty()) { err = errs[j]; return false; }
-      if (!install(dev, srcs[todo[j]], cubins[j], err)) return false;
+      if (!install(dev, keys[todo[j]], srcs[todo[j]], cubins[j], err)) return false;
     }
   }
   std::lock_guard<std::mutex> lk(S.mu);
   for (size_t i = 0; i < passes.size(); ++i)
-    if (!out[i] && !srcs[i].empty()) {
-      auto it = S.cache.find({dev, srcs[i]});
+    if (!out[i]) {
+      auto it = S.cache.find({dev, keys[i]});
       if (it != S.cache.end()) out[i] = it->second.get();
     }
   return true;
@@ -375,15 +378,15 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
   {
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
-      std::string e;
-      std::string src = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
-      if (src.empty()) continue;
-      std::pair<int, std::string> key(dev, std::move(src));
+      std::pair<int, std::string> key(dev, jit_pass_key(*passes[i], min_blocks, threads, set_mode));
       auto it = S.cache.find(key);
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
       if (!queue_missing || S.pending.count(key)) continue;
+      std::string e;
+      std::string src = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
+      if (src.empty()) continue;
       S.pending.insert(key);
-      S.queue.push_back(std::move(key));
+      S.queue.push_back({dev, key.second, std::move(src)});
       queued = true;
     }
     if (queued && S.workers.empty()) {

@@ -230,6 +230,41 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
 
 }  // namespace
 
+// Everything of `d` (and of the kernel form) that its generated source depends
+// on, as a compact byte string: equal keys give equal sources.
+std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode) {
+  std::string k;
+  k.reserve(64 + d.nstages * 32 + d.nops * 16);
+  auto put = [&](uint32_t v) { k.append(reinterpret_cast<const char*>(&v), sizeof(v)); };
+  put(1);   // key format
+  put((uint32_t)min_blocks);
+  put((uint32_t)threads);
+  put(set_mode ? 1u : 0u);
+  put(d.M);
+  put(d.c);
+  put(d.R);
+  put(d.nstages);
+  put(d.mat_elems);
+  put(d.ngrad);
+  for (int s = 0; s < d.nstages; ++s) {
+    const StageDesc& sd = d.st[s];
+    k.append(reinterpret_cast<const char*>(sd.S), kMaxK);
+    k.append(reinterpret_cast<const char*>(sd.lane), kLaneBits);
+    k.push_back((char)sd.nt);
+    k.append(reinterpret_cast<const char*>(sd.tb), sd.nt);
+    put(sd.op0);
+    put(sd.op1);
+  }
+  for (uint32_t i = 0; i < d.nops; ++i) {
+    const OpDesc& o = d.ops[i];
+    const char b[7] = {(char)o.kind, (char)o.a, (char)o.b, (char)o.k, (char)o.perm, (char)o.flags, (char)o.urows};
+    k.append(b, 7);
+    put(o.mat);
+    put(o.gidx);
+  }
+  return k;
+}
+
 // Source of the kernel specialised to pass `d` (see iq_plan.h).
 std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads, bool set_mode) {
   if (!set_mode && (d.ngrad || d.nsets > 1)) {

@@ -318,6 +318,9 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 // parameter block.
 std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2, int threads = 0,
                             bool set_mode = false);
+// Compact byte string of everything jit_pass_source's output depends on
+// (equal keys give equal sources): the kernel cache's key.
+std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode);
 struct cplx64 { double re, im; };
 // Fuse runs of queued operations on at most two qubits into single 4x4 blocks
 // (a two-qubit operation absorbs the open one-qubit blocks of its qubits and
