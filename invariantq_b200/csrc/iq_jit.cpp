@@ -30,6 +30,10 @@ namespace {
 #include "iq_jit_headers.inc"
 
 constexpr int kMaxBufJit = 4;
+// Kernels kept per process.  Modules stay loaded for the process's life (a
+// launch may still use one), so past this many distinct pass structures new
+// passes run on the interpreting kernel.
+constexpr size_t kMaxKernels = 8192;
 
 // ------------------------------------------------------------- NVRTC / driver
 
@@ -336,6 +340,7 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
       keys[i] = jit_pass_key(*passes[i], min_blocks, threads, set_mode);
       auto it = S.cache.find({dev, keys[i]});
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
+      if (S.cache.size() + todo.size() >= kMaxKernels) continue;
       if (!seen.insert(keys[i]).second) continue;
       std::string e;
       srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
@@ -381,7 +386,7 @@ void jit_lookup(const std::vector<const PassDesc*>& passes, std::vector<const Ji
       std::pair<int, std::string> key(dev, jit_pass_key(*passes[i], min_blocks, threads, set_mode));
       auto it = S.cache.find(key);
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
-      if (!queue_missing || S.pending.count(key)) continue;
+      if (!queue_missing || S.pending.count(key) || S.cache.size() + S.pending.size() >= kMaxKernels) continue;
       std::string e;
       std::string src = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
       if (src.empty()) continue;

@@ -102,6 +102,27 @@ struct PassBuilder {
   int lowlimit(const Stage& s, bool no_lanes_after) const {
     return c - kLaneBits + ((no_lanes_after && s.lanereq == 0) ? 1 : 0);
   }
+  // Whether a stage without lane operations whose slots also take the nn bits
+  // `add` keeps three lane candidates with independent swizzle images: the
+  // low three bits of swz(1 << j) are bit j mod 3 for tile-local j < 6 and 0
+  // above, so each class {k, k + 3} (k = 0, 1, 2) needs a member outside the
+  // slots.  Tile-local bits >= c are high tile bits chosen when the pass is
+  // finalised; physical bit j stands in for them (it is the one they are when
+  // it is local in the pass).
+  bool lanes_feasible(const Stage& s, const int* add, int nn) const {
+    for (int k = 0; k < 3; ++k) {
+      bool free_member = false;
+      for (int j = k; j < 6 && !free_member; j += 3) {
+        // j >= c: the high tile bit H[j - c] is at least physical bit j, and is
+        // that bit whenever it is local; count it taken when a slot holds it
+        bool taken = inS(s, j);
+        for (int i = 0; i < nn; ++i) taken |= add[i] == j;
+        free_member = !taken;
+      }
+      if (!free_member) return false;
+    }
+    return true;
+  }
   // Register slots take at most c - 3 of the chunk bits [0, c), so three lane
   // bits always remain inside the chunk; lane operations name up to 3 of them.
   bool tryAdd(Stage& s, const SchedOp& op) const {
@@ -123,7 +144,11 @@ struct PassBuilder {
     for (int i = 0; i < 2; ++i)
       if (!inS(s, op.q[i])) { need[nn++] = op.q[i]; lowadd += op.q[i] < c; }
     if (s.nS + nn > p.R) return false;
-    if (lowcount(s) + lowadd > lowlimit(s, op.grad != 0)) return false;
+    if (lowcount(s) + lowadd > lowlimit(s, op.grad != 0)) {
+      // a stage without lane operations may hold more chunk bits as long as
+      // its lanes can still be drawn with independent swizzle images
+      if (s.lanereq != 0 || !lanes_feasible(s, need, nn)) return false;
+    }
     for (int i = 0; i < nn; ++i) {
       s.S[s.nS++] = need[i];
       s.lanereq &= ~(1ULL << need[i]);   // earlier lane ops on this bit become slot ops

@@ -559,3 +559,94 @@ extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int*
   memcpy(out, all.c_str(), all.size() + 1);
   return count;
 }
+
+// Human-readable stage layout of every planned pass (development aid for the
+// planner): per stage the physical bits of the register slots and lanes and
+// the operations (kind, slot/lane a, slot b).
+extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, double budget, int fuse, int nops,
+                             const int* ks, const int* qs, const double* mats, const long long* mat_off, char* out,
+                             long long outlen) {
+  std::vector<cd> pool;
+  std::vector<SchedOp> ops;
+  for (int i = 0; i < nops; ++i) {
+    SchedOp o{};
+    o.k = (uint8_t)ks[i];
+    for (int j = 0; j < ks[i]; ++j) o.q[j] = (uint8_t)qs[i * 5 + j];
+    const int d = 1 << ks[i];
+    const double* m = mats + 2 * mat_off[i];
+    o.mat = (uint32_t)pool.size();
+    o.dense = o.mat;
+    for (int j = 0; j < d * d; ++j) pool.emplace_back(m[2 * j], m[2 * j + 1]);
+    double ph[8];
+    uint8_t perm = 0, unit = 0;
+    if (ks[i] <= 2 && classify_monomial(m, ks[i], &perm, ph, &unit)) {
+      o.mono = 1;
+      o.perm = perm;
+      o.unit = unit;
+      o.mat = (uint32_t)pool.size();
+      for (int j = 0; j < d; ++j) pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    }
+    ops.push_back(o);
+  }
+  std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(pool.data()),
+                         reinterpret_cast<const cplx64*>(pool.data()) + pool.size());
+  if (fuse) ops = fuse_two_qubit_blocks(ops, cp, fuse == 2);
+  if (fuse == 2) {
+    decompose_one_qubit_ops(ops, cp);
+    normalize_one_qubit_ops(ops, cp);
+  }
+  SchedParams p{};
+  p.nbits = nbits;
+  p.M = M;
+  p.c = c;
+  p.R = R;
+  p.max_stages = max_stages;
+  p.budget = budget;
+  std::vector<PassPlan> plans;
+  std::string err, all;
+  if (plan_passes(p, ops, plans, err) < 0) {
+    snprintf(out, (size_t)outlen, "plan: %s", err.c_str());
+    return -1;
+  }
+  static const char* kind[] = {"-", "D1R", "D1L", "D2R", "DKR", "M1R", "M1L", "M2R", "G2", "N1R", "R1R"};
+  char buf[256];
+  for (size_t pi = 0; pi < plans.size(); ++pi) {
+    const PassDesc& d = plans[pi].desc;
+    auto phys = [&](int j) { return j < d.c ? j : (int)d.H[j - d.c]; };
+    snprintf(buf, sizeof buf, "pass %zu cost %.0f stages %d ops %u\n", pi, plans[pi].cost, d.nstages, d.nops);
+    all += buf;
+    for (int s = 0; s < d.nstages; ++s) {
+      const StageDesc& sd = d.st[s];
+      all += "  S[";
+      for (int i = 0; i < d.R; ++i) { snprintf(buf, sizeof buf, "%d%s", phys(sd.S[i]), i + 1 < d.R ? " " : ""); all += buf; }
+      all += "] L[";
+      for (int i = 0; i < kLaneBits; ++i) { snprintf(buf, sizeof buf, "%d%s", phys(sd.lane[i]), i + 1 < kLaneBits ? " " : ""); all += buf; }
+      uint32_t v[3], r = 0;
+      for (int i = 0; i < 3; ++i) v[i] = swz(1u << sd.lane[i]) & 7u;
+      for (int bit = 0; bit < 3; ++bit) {   // rank over GF(2) of the lanes' swizzle images
+        int piv = -1;
+        for (int i = (int)r; i < 3; ++i)
+          if ((v[i] >> bit) & 1) { piv = i; break; }
+        if (piv < 0) continue;
+        std::swap(v[r], v[piv]);
+        for (int i = 0; i < 3; ++i)
+          if (i != (int)r && ((v[i] >> bit) & 1)) v[i] ^= v[r];
+        ++r;
+      }
+      snprintf(buf, sizeof buf, "] rank%u", r);
+      all += buf;
+      for (int o = sd.op0; o < sd.op1; ++o) {
+        const OpDesc& od = d.ops[o];
+        if (od.k == 2) snprintf(buf, sizeof buf, " %s(%d,%d)", kind[od.kind], phys(sd.S[od.a]), phys(sd.S[od.b]));
+        else if (od.kind == OP_D1L || od.kind == OP_M1L) snprintf(buf, sizeof buf, " %s(L%d)", kind[od.kind], phys(sd.lane[od.a]));
+        else if (od.kind == OP_DKR) snprintf(buf, sizeof buf, " DKR%d", od.k);
+        else snprintf(buf, sizeof buf, " %s(%d)", kind[od.kind], phys(sd.S[od.a]));
+        all += buf;
+      }
+      all += "\n";
+    }
+  }
+  if ((long long)all.size() + 1 > outlen) return -1;
+  memcpy(out, all.c_str(), all.size() + 1);
+  return (int)plans.size();
+}
