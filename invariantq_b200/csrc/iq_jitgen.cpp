@@ -105,6 +105,17 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         }
         break;
       }
+      case OP_R1L: {   // normalised rotation on a lane bit
+        const int l = od.a;
+        const std::string hi = g.fresh();
+        const std::string w = od.perm ? mat(m + 0) + ".x" : mat(m + 2) + ".x";
+        o << "        const bool " << hi << " = (lane8 >> " << l << ") & 1;\n";
+        for (int v = 0; v < NV; ++v) {
+          const std::string p = def("shfl_xor2(" + cur[v] + ", " + std::to_string(1 << l) + ", omask)");
+          cur[v] = def("rot_lane<" + std::string(od.perm ? "1" : "0") + ">(" + w + ", " + hi + ", " + cur[v] + ", " + p + ")");
+        }
+        break;
+      }
       case OP_M1R: {
         const int A = 1 << od.a;
         const bool sw = od.perm & 1;

@@ -153,6 +153,18 @@ __device__ __forceinline__ double2 rot_row1(double w, double2 x, double2 y) {
                    : make_double2(fma(w, y.x, x.x), fma(w, y.y, x.y));
 }
 
+// a normalised rotation on a lane bit: own amplitude x, partner's p, hi = this
+// lane's value of the bit.  FORM 0: y = x + (hi ? w : -w) p; FORM 1:
+// y = w x + (hi ? p : -p)
+template <int FORM>
+__device__ __forceinline__ double2 rot_lane(double w, bool hi, double2 x, double2 p) {
+  if (FORM == 0) {
+    const double c = hi ? w : -w;
+    return make_double2(fma(c, p.x, x.x), fma(c, p.y, x.y));
+  }
+  return make_double2(fma(w, x.x, hi ? p.x : -p.x), fma(w, x.y, hi ? p.y : -p.y));
+}
+
 __device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
   return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
 }

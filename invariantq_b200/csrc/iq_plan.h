@@ -77,6 +77,8 @@ enum OpKind : uint8_t {
   OP_R1R = 10,  // real rotation on register slot a, normalised (2 FMAs per amplitude): perm 0:
                 // [[1, -t], [t, 1]] with t = Re m[2]; perm 1: [[u, -1], [1, u]] with u = Re m[0];
                 // stored whole, so a lane placement runs it as OP_D1L
+  OP_R1L = 11,  // the same rotation on lane bit a: each lane combines its own amplitude with its
+                // partner's (warp shuffle): 2 FMAs per amplitude in the tan form
 };
 
 // flags

@@ -454,7 +454,11 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
             if (o.norm) od.perm = (uint8_t)(o.norm - 1);
             if (o.rot) od.perm = (uint8_t)(o.rot - 1);
           }
-          else if (lane_of[j] >= 0) { od.kind = o.mono ? OP_M1L : OP_D1L; od.a = (uint8_t)lane_of[j]; }
+          else if (lane_of[j] >= 0) {
+            od.kind = o.mono ? OP_M1L : (o.rot ? OP_R1L : OP_D1L);
+            od.a = (uint8_t)lane_of[j];
+            if (o.rot) od.perm = (uint8_t)(o.rot - 1);
+          }
           else { err = "internal: 1q operation bit is neither a slot nor a lane"; return -1; }
         } else if (o.k == 2) {
           const int j0 = pos[o.q[0]], j1 = pos[o.q[1]];

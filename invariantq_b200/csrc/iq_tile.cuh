@@ -294,6 +294,19 @@ __device__ __forceinline__ void d1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
+template <int R, int FORM>
+__device__ __forceinline__ void r1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
+                                    int lane8, unsigned omask) {
+  const bool hi = (lane8 >> lb) & 1;
+  const double w = FORM == 0 ? ld_mat(m, 2).x : ld_mat(m, 0).x;
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    const double2 x = s[v];
+    const double2 p = shfl_xor2(x, 1 << lb, omask);
+    d[v] = rot_lane<FORM>(w, hi, x, p);
+  }
+}
+
 template <int R>
 __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
                                     int lane8, unsigned omask, int perm, bool unit) {
@@ -441,6 +454,10 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
     case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
     case OP_N1R: disp_n1r<R>(od.a, od.perm, s, d, m); break;
     case OP_R1R: disp_r1r<R>(od.a, od.perm, s, d, m); break;
+    case OP_R1L:
+      if (od.perm) r1l<R, 1>(s, d, m, od.a, lane8, omask);
+      else r1l<R, 0>(s, d, m, od.a, lane8, omask);
+      break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
     case OP_D2R:
       // one jump over the ordered slot pair (a, b) instead of nested compares

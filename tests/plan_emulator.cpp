@@ -109,7 +109,8 @@ struct Emu {
                 a[L][v | (1 << od.a)] = mat(od.mat, 2) * x + mat(od.mat, 3) * y;
               }
             break;
-          case OP_D1L: {
+          case OP_D1L:
+          case OP_R1L: {   // the rotation's matrix is stored whole
             auto old = a;
             for (int L = 0; L < 8; ++L) {
               const int my = (L >> od.a) & 1, pl = L ^ (1 << od.a);
