@@ -147,7 +147,11 @@ size_t iq_statevector_num_qubits(void* sv);
  * "plan_style" (0: follow "jit"; 1: plan for the interpreting kernel, fusing
  * one-qubit gates into two-qubit blocks; 2: plan for specialised kernels,
  * leaving CX/CZ/SWAP apart and normalising dense one-qubit gates), "normalize"
- * (1: normalised one-qubit gates in plans of style 2).
+ * (1: normalised one-qubit gates in plans of style 2).  Plans of style 2 run
+ * 4 CTAs per SM with one tile buffer unless those options (or IQ_CTAS_PER_SM,
+ * IQ_NBUF) are set; get_option reports the values the handle's next plan
+ * uses.  "chunk_bits" 3 with "budget" 160 plans fewer, fuller passes: a
+ * faster circuit at a lower bandwidth per pass.
  * 0 = ok, -1 = unknown key or bad value. */
 int iq_handle_set_option(void* h, const char* key, double value);
 double iq_handle_get_option(void* h, const char* key);

@@ -29,7 +29,7 @@ import numpy as np
 from .fusion import GateFusionPass
 from .ir import CircuitIR, op_kind
 
-DEFAULT_CANDIDATES = {"k": (2, 3, 4), "tile_bits": (11, 12), "budget": (48, 80, 128), "reg_slots": (4,)}
+DEFAULT_CANDIDATES = {"k": (2, 3, 4), "tile_bits": (11, 12), "budget": (80, 120, 160), "reg_slots": (4,)}
 
 
 def default_cache_path() -> Path:

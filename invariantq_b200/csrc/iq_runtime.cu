@@ -215,6 +215,25 @@ struct Engine {
   int normalize = 1;   // normalised one-qubit operations in specialised passes
   int plan_style = 0;  // 0: by the jit setting; 1: as for the interpreting kernel; 2: as for specialised kernels
   int jit_threads = 0; // CTA size of specialised kernels (0: by register slots; 128 or 256)
+  // settings given explicitly (option or environment); the others take the
+  // defaults of the plan style: specialised kernels run 4 CTAs per SM with one
+  // tile buffer each (measured best on the 30-qubit brick-wall)
+  bool set_c = false, set_budget = false, set_nbuf = false, set_ctas = false;
+
+  bool spec_style() const {
+    return plan_style == 2 || (plan_style == 0 && jit && (jit >= 2 || nbits >= kJitMinBits) && !eager && nbits >= 7);
+  }
+  SchedParams plan_params(bool spec) const {
+    SchedParams p = sp;
+    (void)spec;
+    return p;
+  }
+  TileLaunch launch_params(bool spec) const {
+    TileLaunch t = tl;
+    if (spec && !set_ctas) t.ctas_per_sm = 4;
+    if (spec && !set_nbuf) t.nbuf = 1;
+    return t;
+  }
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof;
 
   double st_passes = 0, st_ops = 0, st_bytes = 0, st_launches = 0, st_flushes = 0, st_tile = 0, st_h2d = 0;
@@ -265,6 +284,10 @@ struct Engine {
     sp.budget = env_double("IQ_PASS_BUDGET", 120.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
     tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
+    set_c = getenv("IQ_CHUNK_BITS") != nullptr;
+    set_budget = getenv("IQ_PASS_BUDGET") != nullptr;
+    set_nbuf = getenv("IQ_NBUF") != nullptr;
+    set_ctas = getenv("IQ_CTAS_PER_SM") != nullptr;
     eager = env_int("IQ_EAGER", 0);
     return reset_state();
   }
@@ -397,6 +420,7 @@ struct Engine {
     int nops = 0;
     std::vector<const JitKernel*> jit;   // specialised kernel per pass (null: interpreting kernel)
     std::vector<cplx64> hmats;           // host copy of the pass matrix blocks (launch parameters)
+    TileLaunch tl{};                     // launch settings of the passes
   };
 
   // kernels specialised to the program's passes: compiled now (recorded
@@ -407,12 +431,12 @@ struct Engine {
     for (auto& pl : pg.plans) ds.push_back(&pl.desc);
     if (own || jit >= 2) {
       std::string err;
-      if (!jit_prepare(ds, pg.jit, err, tl.ctas_per_sm, jit_threads)) {
+      if (!jit_prepare(ds, pg.jit, err, pg.tl.ctas_per_sm, jit_threads)) {
         jit_note(err);
         pg.jit.clear();
       }
     } else {
-      jit_lookup(ds, pg.jit, true, tl.ctas_per_sm, jit_threads);
+      jit_lookup(ds, pg.jit, true, pg.tl.ctas_per_sm, jit_threads);
     }
     bool any = false;
     for (auto* k : pg.jit) any |= k != nullptr;
@@ -424,8 +448,8 @@ struct Engine {
     pg.nops = (int)ops.size();
     // passes that specialised kernels will run: two-qubit monomials stay apart
     // (renamings there) and dense one-qubit operations are normalised
-    const bool spec = plan_style == 2 ||
-                      (plan_style == 0 && jit && (jit >= 2 || nbits >= kJitMinBits) && !eager && nbits >= 7);
+    const bool spec = spec_style();
+    pg.tl = launch_params(spec);
     std::vector<SchedOp> fused = fuse ? fuse_two_qubit_blocks(ops, pool, spec) : ops;
     if (spec && normalize) {
       decompose_one_qubit_ops(fused, pool);
@@ -446,7 +470,7 @@ struct Engine {
         pg.sops.push_back(so);
       }
     } else {
-      SchedParams p = sp;
+      SchedParams p = plan_params(spec);
       p.nbits = nbits;
       p.R = std::min(5, std::max(sp.R, maxk));
       std::string err;
@@ -504,12 +528,12 @@ struct Engine {
       const PassDesc& desc = pg.plans[i].desc;
       if (i < pg.jit.size() && pg.jit[i]) {
         if (!cuda_ok(jit_launch(pg.jit[i], pg.tmaps[i], desc,
-                                reinterpret_cast<const double2*>(pg.hmats.data()) + desc.mat_base, d_status, tl,
+                                reinterpret_cast<const double2*>(pg.hmats.data()) + desc.mat_base, d_status, pg.tl,
                                 num_sms, stream),
                      "specialised tile pass kernel"))
           return false;
         ++st_jit;
-      } else if (!cuda_ok(launch_tile_pass(pg.tmaps[i], desc, pg.d_mats, d_status, tl, num_sms, stream),
+      } else if (!cuda_ok(launch_tile_pass(pg.tmaps[i], desc, pg.d_mats, d_status, pg.tl, num_sms, stream),
                           "tile pass kernel")) {
         return false;
       }
@@ -1116,12 +1140,12 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   if (!e->flush()) return -1;
   const int iv = (int)v;
   if (!strcmp(key, "tile_bits")) { if (iv < 7 || iv > kMaxTileBits) return -1; e->sp.M = iv; }
-  else if (!strcmp(key, "chunk_bits")) { if (iv < 5 || iv > 7) return -1; e->sp.c = iv; }
+  else if (!strcmp(key, "chunk_bits")) { if (iv < 3 || iv > 7) return -1; e->sp.c = iv; e->set_c = true; }
   else if (!strcmp(key, "max_stages")) { if (iv < 1 || iv > kMaxStages) return -1; e->sp.max_stages = iv; }
-  else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; }
-  else if (!strcmp(key, "nbuf")) { if (iv < 1 || iv > 4) return -1; e->tl.nbuf = iv; }
+  else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; e->set_budget = true; }
+  else if (!strcmp(key, "nbuf")) { if (iv < 1 || iv > 4) return -1; e->tl.nbuf = iv; e->set_nbuf = true; }
   else if (!strcmp(key, "reg_slots")) { if (iv < 3 || iv > 5) return -1; e->sp.R = iv; }
-  else if (!strcmp(key, "ctas_per_sm")) { if (iv < 1 || iv > 4) return -1; e->tl.ctas_per_sm = iv; }
+  else if (!strcmp(key, "ctas_per_sm")) { if (iv < 1 || iv > 4) return -1; e->tl.ctas_per_sm = iv; e->set_ctas = true; }
   else if (!strcmp(key, "consumers")) { if (iv != 128) return -1; e->tl.consumers = iv; }
   else if (!strcmp(key, "eager")) e->eager = iv ? 1 : 0;
   else if (!strcmp(key, "fuse")) e->fuse = iv ? 1 : 0;
@@ -1145,12 +1169,14 @@ double iq_handle_get_option(void* h, const char* key) {
   Engine* e = static_cast<Engine*>(h);
   if (!e || !key) return kNaN;
   if (!strcmp(key, "tile_bits")) return e->sp.M;
-  if (!strcmp(key, "chunk_bits")) return e->sp.c;
+  // the values the handle's next plan uses (its plan style's defaults where not set)
+  const bool spec = e->spec_style();
+  if (!strcmp(key, "chunk_bits")) return e->plan_params(spec).c;
   if (!strcmp(key, "max_stages")) return e->sp.max_stages;
-  if (!strcmp(key, "budget")) return e->sp.budget;
-  if (!strcmp(key, "nbuf")) return e->tl.nbuf;
+  if (!strcmp(key, "budget")) return e->plan_params(spec).budget;
+  if (!strcmp(key, "nbuf")) return e->launch_params(spec).nbuf;
   if (!strcmp(key, "reg_slots")) return e->sp.R;
-  if (!strcmp(key, "ctas_per_sm")) return e->tl.ctas_per_sm;
+  if (!strcmp(key, "ctas_per_sm")) return e->launch_params(spec).ctas_per_sm;
   if (!strcmp(key, "consumers")) return e->tl.consumers;
   if (!strcmp(key, "eager")) return e->eager;
   if (!strcmp(key, "fuse")) return e->fuse;

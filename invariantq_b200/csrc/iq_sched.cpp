@@ -146,8 +146,10 @@ struct PassBuilder {
     if (s.nS + nn > p.R) return false;
     if (lowcount(s) + lowadd > lowlimit(s, op.grad != 0)) {
       // a stage without lane operations may hold more chunk bits as long as
-      // its lanes can still be drawn with independent swizzle images
-      if (s.lanereq != 0 || !lanes_feasible(s, need, nn)) return false;
+      // its lanes can still be drawn with independent swizzle images; an empty
+      // stage takes the operation regardless (its lanes may then share bank
+      // groups: slower, still correct)
+      if (s.lanereq != 0 || (s.nS > 0 && !lanes_feasible(s, need, nn))) return false;
     }
     for (int i = 0; i < nn; ++i) {
       s.S[s.nS++] = need[i];
@@ -275,7 +277,9 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
   const bool whole = nb <= p.M;         // the whole array is one tile
   const int c = whole ? std::min(p.c, M) : p.c;
   if (M < p.R + kLaneBits || M > kMaxTileBits) { err = "tile bits out of range"; return -1; }
-  if (c < 5 || c > 7) { err = "chunk bits must be 5..7"; return -1; }
+  if (c < 3 || c > 7) { err = "chunk bits must be 3..7"; return -1; }
+  // a tile moves in 2^(M - c - 2) box copies, one per lane of the CTA's first 128 threads
+  if (!whole && M - c - 2 > 7) { err = "too many tile copies: raise the chunk bits or lower the tile bits"; return -1; }
   if (!whole && M - c < kMaxK) { err = "tile must hold the chunk plus 5 free bits"; return -1; }
 
   for (int i = 0; i < nops; ++i) {

@@ -609,7 +609,7 @@ extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, dou
     snprintf(out, (size_t)outlen, "plan: %s", err.c_str());
     return -1;
   }
-  static const char* kind[] = {"-", "D1R", "D1L", "D2R", "DKR", "M1R", "M1L", "M2R", "G2", "N1R", "R1R"};
+  static const char* kind[] = {"-", "D1R", "D1L", "D2R", "DKR", "M1R", "M1L", "M2R", "G2", "N1R", "R1R", "R1L"};
   char buf[256];
   for (size_t pi = 0; pi < plans.size(); ++pi) {
     const PassDesc& d = plans[pi].desc;
@@ -639,7 +639,7 @@ extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, dou
       for (int o = sd.op0; o < sd.op1; ++o) {
         const OpDesc& od = d.ops[o];
         if (od.k == 2) snprintf(buf, sizeof buf, " %s(%d,%d)", kind[od.kind], phys(sd.S[od.a]), phys(sd.S[od.b]));
-        else if (od.kind == OP_D1L || od.kind == OP_M1L) snprintf(buf, sizeof buf, " %s(L%d)", kind[od.kind], phys(sd.lane[od.a]));
+        else if (od.kind == OP_D1L || od.kind == OP_M1L || od.kind == OP_R1L) snprintf(buf, sizeof buf, " %s(L%d)", kind[od.kind], phys(sd.lane[od.a]));
         else if (od.kind == OP_DKR) snprintf(buf, sizeof buf, " DKR%d", od.k);
         else snprintf(buf, sizeof buf, " %s(%d)", kind[od.kind], phys(sd.S[od.a]));
         all += buf;

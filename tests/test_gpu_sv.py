@@ -114,7 +114,8 @@ def test_random_sequences_vs_oracle(SV, port, n, seed, eager):
 
 
 @pytest.mark.parametrize("M,c,budget,stages,nbuf", [(12, 5, 80, 8, 3), (11, 6, 40, 4, 2), (13, 5, 200, 8, 1),
-                                                    (10, 5, 16, 2, 4), (12, 7, 500, 16, 2)])
+                                                    (10, 5, 16, 2, 4), (12, 7, 500, 16, 2), (11, 3, 120, 8, 3),
+                                                    (12, 3, 80, 6, 3), (11, 4, 120, 8, 3)])
 def test_tile_configurations(SV, port, M, c, budget, stages, nbuf):
     n = 18
     rng = np.random.default_rng(M * 100 + c)

@@ -129,6 +129,9 @@ def oracle_apply(port, state, n, ops):
     (10, 10, 5, 3, 8, 80.0, 9),     # three register slots (256-thread variant)
     (13, 11, 5, 3, 6, 60.0, 10),
     (14, 11, 6, 3, 8, 120.0, 11),
+    (14, 11, 3, 4, 8, 120.0, 12),   # three chunk bits: more high tile bits per pass
+    (15, 12, 3, 4, 6, 80.0, 13),
+    (13, 11, 4, 4, 8, 96.0, 14),
 ])
 def test_emulated_passes_match_oracle(port, emu, n, M, c, R, stages, budget, seed):
     rng = np.random.default_rng(seed)
