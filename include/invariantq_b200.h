@@ -191,10 +191,16 @@ int iq_handle_profile_read(void* h, double* ms_out, size_t max);
  * code running inside another framework that owns the free device memory.  Its
  * reduction scratch is a fixed array in the library (about 166 KB per GPU,
  * held until the process exits), so num_qubits is limited to
- * IQ_NOALLOC_MAX_QUBITS and larger sizes are rejected with an error.  The
- * first call on each device looks up that array's device address once; make
- * that first call before any stream capture.  All calls on one device share
- * the array, so calls that overlap on the GPU (different streams, no ordering
+ * IQ_NOALLOC_MAX_QUBITS and larger sizes are rejected with an error.  d_amps
+ * may be device or managed memory; the call runs on the device that holds it
+ * and leaves the caller's current device as it found it.  The first call on
+ * each device does a one-time set-up: it loads the call's kernels (with CUDA's
+ * default lazy module loading, code is loaded into device memory at first use)
+ * and looks up the scratch array's device address.  Make that first call before
+ * the device memory is committed and before any stream capture; later calls
+ * take no device memory.  A cudaDeviceReset invalidates the set-up (the looked-up
+ * address belongs to the context it ends).  All calls on one device share the
+ * array, so calls that overlap on the GPU (different streams, no ordering
  * between them) race and must be avoided.  Returns 0, or -1 with iq_last_error
  * set. */
 #define IQ_NOALLOC_MAX_QUBITS 34

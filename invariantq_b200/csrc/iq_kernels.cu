@@ -358,6 +358,13 @@ cudaError_t launch_zsums(const double2* s, int nbits, double* partials, double* 
   return cudaGetLastError();
 }
 
+cudaError_t preload_zsums() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, zsums_kernel);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, zsums_final_kernel);
+  return e;
+}
+
 // ------------------------------------------------------------ elementwise
 
 __global__ void collapse_kernel(double2* __restrict__ s, uint64_t dim, uint64_t mask, uint64_t val, double f) {

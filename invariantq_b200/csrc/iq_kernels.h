@@ -57,6 +57,10 @@ cudaError_t launch_pauli_sum(const double2* s, uint64_t dim, uint64_t xmask, uin
                              double2* partials, double2* out, cudaStream_t st);
 // out[0] = sum |a|^2, out[1 + b] = sum over i with bit b set of |a_i|^2, b < nbits
 cudaError_t launch_zsums(const double2* s, int nbits, double* partials, double* out, cudaStream_t st);
+// Loads the two kernels of launch_zsums on the current device now (under lazy
+// module loading they would otherwise load, and take device memory for their
+// code, at their first launch).
+cudaError_t preload_zsums();
 size_t zsums_partials_doubles(int nbits);
 
 // ---- elementwise ----
@@ -96,6 +100,13 @@ cudaError_t launch_hamiltonian_joint(const double2* psi, int n, int nsets, uint6
                                      const uint64_t* zmask, const double2* coef, double2* joint, double* partials,
                                      double* energy, cudaStream_t st);
 cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st);
+
+// Eigenvalues (ascending) of the reduced state on the kept qubits keep[0..k) of
+// the 2^nbits state psi, computed on the device (iq_entropy.cu); k is at most
+// reduced_spectrum_max_bits() and below nbits.  Synchronises `st`.
+int reduced_spectrum_max_bits();
+cudaError_t reduced_spectrum(const double2* psi, int nbits, const int* keep, int k, std::vector<double>& eig,
+                             cudaStream_t st);
 
 // Record an error for iq_last_error (defined in iq_runtime.cu).
 void record_error(int code, const char* msg);
