@@ -34,11 +34,14 @@ _vp = ctypes.c_void_p
 _sz = ctypes.c_size_t
 
 
-def build(ref: bool = False) -> None:
-    """Compile the C restatement (and, if asked and the sources exist, the reference core)."""
+def build(ref: bool = False, ref_dir: Optional[str] = None) -> None:
+    """Compile the C restatement and, if asked and a reference checkout is named
+    (``ref_dir`` or the environment variable IQ_REFERENCE_DIR) and holds the
+    core sources, the reference core into oracle/_ref."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if ref and Path(os.environ.get("IQ_REFERENCE_DIR", "/root/reference"), "core").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    src = ref_dir or os.environ.get("IQ_REFERENCE_DIR")
+    if ref and src and Path(src, "core").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={src}"], check=True)
 
 
 def _dptr(a: np.ndarray):

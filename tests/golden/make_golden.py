@@ -3,7 +3,8 @@
 Run where the reference sources exist (they do not travel to the GPU machine):
 
     make -C oracle ref            # builds oracle/_ref/libinvariantq.so from the reference sources
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
+                                        # or IQ_REFERENCE_DIR=<reference checkout>
 
 The script copies the reference's Python package into a temporary directory,
 drops the reference core built by ``oracle/Makefile`` next to its ctypes
@@ -21,6 +22,14 @@ and records what the reference's own code returns:
                           and the Kraus sets of ``channels.py:11-103``.
 * ``simulators.npz``   -- ``StateVectorSimulator.run`` / ``DensityMatrixSimulator.run``
                           on seeded circuits (including the brick-wall U3+CX workload).
+* ``binding_argtypes.json`` -- the ctypes signature the reference's binding sets on
+                          each of the 49 C-ABI functions (binding.py:54-299).
+* ``abi_traces.json``  -- every C-ABI call the reference's own tests make
+                          (tests/test_core_math.py:10-69,
+                          tests/test_independent_reference.py:15-61) when run on
+                          the reference core through its unmodified binding and
+                          drivers: arguments, and the values the core returned,
+                          for a replay against another library.
 
 Every input is seeded; the fixtures are small (kilobytes).
 """
@@ -29,6 +38,7 @@ from __future__ import annotations
 import argparse
 import importlib
 import math
+import os
 import shutil
 import sys
 import tempfile
@@ -308,6 +318,158 @@ def gen_simulators(iq, out):
     np.savez_compressed(out / "simulators.npz", **d)
 
 
+# ---------------------------------------------------------------- C-ABI traces
+
+def _ctype_name(t):
+    if t is None:
+        return None
+    return t.__name__
+
+
+def gen_binding_argtypes(binding, out):
+    """argtypes / restype the reference binding sets on every exported function."""
+    import json
+    names = (out / "c_api_symbols.txt").read_text().split()
+    table = {}
+    for name in names:
+        fn = getattr(binding._NATIVE_LIB, name)
+        table[name] = {"argtypes": [_ctype_name(t) for t in (fn.argtypes or [])], "restype": _ctype_name(fn.restype)}
+    (out / "binding_argtypes.json").write_text(json.dumps(table, indent=1, sort_keys=True) + "\n")
+
+
+class _Tracer:
+    """Stands in for the binding's ``_NATIVE_LIB``: forwards every call to the
+    reference core and records the state-vector and density-matrix calls with
+    their input arrays and the values the core returned."""
+
+    # pointer arguments: (index, kind, length rule); kinds: din (double input),
+    # zin (size_t input), dout / uout (double / uint64 output), ref (double by reference)
+    SPEC = {
+        "iq_statevector_apply_1q": [(2, "din", lambda a, n: 4), (3, "din", lambda a, n: 4)],
+        "iq_statevector_apply_2q": [(3, "din", lambda a, n: 16), (4, "din", lambda a, n: 16)],
+        "iq_statevector_apply_fused": [(1, "zin", lambda a, n: a[2]), (3, "din", lambda a, n: 4 ** a[2]),
+                                       (4, "din", lambda a, n: 4 ** a[2])],
+        "iq_statevector_get_amplitudes": [(1, "dout", lambda a, n: 1 << n), (2, "dout", lambda a, n: 1 << n)],
+        "iq_statevector_get_probabilities": [(1, "dout", lambda a, n: 1 << n)],
+        "iq_statevector_sample": [(3, "uout", lambda a, n: a[1])],
+        "iq_statevector_entropy": [(1, "zin", lambda a, n: a[2])],
+        "iq_statevector_expval_pauli": [(2, "zin", lambda a, n: a[3]), (4, "ref", None), (5, "ref", None)],
+        "iq_density_matrix_apply_1q_unitary": [(2, "din", lambda a, n: 4), (3, "din", lambda a, n: 4)],
+        "iq_density_matrix_apply_2q_unitary": [(3, "din", lambda a, n: 16), (4, "din", lambda a, n: 16)],
+        "iq_density_matrix_apply_kraus_1q": [(3, "din", lambda a, n: 4 * a[2]), (4, "din", lambda a, n: 4 * a[2])],
+        "iq_density_matrix_get_elements": [(1, "dout", lambda a, n: 1 << (2 * n)),
+                                           (2, "dout", lambda a, n: 1 << (2 * n))],
+    }
+
+    def __init__(self, lib):
+        self._lib = lib
+        self.calls = []
+        self.handles = {}      # core pointer -> (id, qubits)
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+        if not (name.startswith("iq_statevector_") or name.startswith("iq_density_matrix_")):
+            return fn
+        tracer = self
+
+        def call(*args):
+            return tracer._call(name, fn, args)
+        return call
+
+    def _call(self, name, fn, args):
+        import ctypes
+        args = list(args)
+        spec = {i: (kind, rule) for i, kind, rule in self.SPEC.get(name, [])}
+        rec_args = []
+        if name.endswith("_create"):
+            n = int(args[0])
+        else:
+            hid, n = self.handles[int(args[0])]
+        plain = [a if not isinstance(a, (int, float)) else a for a in args]
+        for i, a in enumerate(args):
+            if i == 0 and not name.endswith("_create"):
+                rec_args.append({"h": hid})
+            elif i in spec:
+                kind, rule = spec[i]
+                if kind in ("din", "zin"):
+                    L = int(rule(plain, n))
+                    ct = ctypes.c_double if kind == "din" else ctypes.c_size_t
+                    arr = np.ctypeslib.as_array(ctypes.cast(a, ctypes.POINTER(ct)), shape=(L,)).copy()
+                    rec_args.append({kind: arr.tolist()})
+                elif kind in ("dout", "uout"):
+                    rec_args.append({kind: int(rule(plain, n))})
+                else:
+                    rec_args.append({"ref": 1})
+            elif isinstance(a, bytes):
+                rec_args.append({"s": a.decode("ascii")})
+            elif isinstance(a, float):
+                rec_args.append(a)
+            else:
+                rec_args.append(int(a))
+        ret = fn(*args)
+        rec = {"fn": name, "args": rec_args}
+        outs = {}
+        for i, (kind, rule) in spec.items():
+            if kind in ("dout", "uout"):
+                L = int(rule(plain, n))
+                ct = ctypes.c_double if kind == "dout" else ctypes.c_uint64
+                arr = np.ctypeslib.as_array(ctypes.cast(args[i], ctypes.POINTER(ct)), shape=(L,)).copy()
+                outs[str(i)] = arr.tolist() if kind == "dout" else [int(x) for x in arr]
+            elif kind == "ref":
+                outs[str(i)] = float(args[i]._obj.value)
+        if outs:
+            rec["out"] = outs
+        if name.endswith("_create"):
+            hid = len(self.handles)
+            self.handles[int(ret)] = (hid, n)
+            rec["ret"] = {"h": hid}
+        elif ret is not None:
+            rec["ret"] = ret if isinstance(ret, float) else int(ret)
+        self.calls.append(rec)
+        return ret
+
+
+def gen_abi_traces(binding, ref_dir: Path, out: Path):
+    """Run the reference's own tests that pin this path (their functions called
+    as written, on the reference core, through the unmodified binding and
+    drivers) with the binding's library replaced by a tracer, and store each
+    test's C-ABI call sequence with the core's results.  The independent
+    einsum reference's state vectors (independent_reference.py:13-73) are kept
+    beside the traces of the tests that compare against them."""
+    import json
+    tests_dir = ref_dir / "tests"
+    sys.path.insert(0, str(tests_dir))
+    scenarios = []
+    real = binding._NATIVE_LIB
+    try:
+        for mod_name, funcs in (("test_core_math", ["test_single_qubit_gates", "test_bell_state_entanglement",
+                                                     "test_product_state_zero_entropy",
+                                                     "test_pauli_expectation_values", "test_measurement_collapse"]),
+                                ("test_independent_reference", ["test_independent_reference_ghz",
+                                                                "test_independent_reference_random_circuits",
+                                                                "test_independent_reference_against_density_matrix"])):
+            mod = importlib.import_module(mod_name)
+            for f in funcs:
+                tracer = _Tracer(real)
+                binding._NATIVE_LIB = tracer
+                try:
+                    getattr(mod, f)()
+                finally:
+                    binding._NATIVE_LIB = real
+                scenarios.append({"test": f"{mod_name}.py::{f}", "calls": tracer.calls})
+    finally:
+        sys.path.remove(str(tests_dir))
+    # the independent reference's states for the circuits those tests build
+    from invariantq.benchmarks.suite import create_random_circuit, create_ghz_circuit  # noqa: E402
+    from invariantq.verification.independent_reference import run_independent_reference  # noqa: E402
+    indep = {"ghz4": run_independent_reference(create_ghz_circuit(4))}
+    for seed in range(5):
+        indep[f"random4_s{seed}"] = run_independent_reference(create_random_circuit(num_qubits=4, depth=6, seed=seed))
+    doc = {"scenarios": scenarios,
+           "independent": {k: {"re": np.real(v).tolist(), "im": np.imag(v).tolist()} for k, v in indep.items()}}
+    (out / "abi_traces.json").write_text(json.dumps(doc) + "\n")
+
+
 def gen_symbols(ref_dir: Path, out: Path):
     """The exported function names of the reference C ABI (core/include/c_api.h)."""
     import re
@@ -318,9 +480,12 @@ def gen_symbols(ref_dir: Path, out: Path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("IQ_REFERENCE_DIR"),
+                    help="the reference checkout (default: $IQ_REFERENCE_DIR)")
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
+    if not a.reference:
+        raise SystemExit("give the reference checkout with --reference or IQ_REFERENCE_DIR")
     out = Path(a.out)
     with tempfile.TemporaryDirectory() as td:
         iq, binding = load_reference(Path(a.reference), Path(td))
@@ -329,7 +494,9 @@ def main():
         gen_dm_ops(iq, binding, out)
         gen_gates(iq, out)
         gen_simulators(iq, out)
-    gen_symbols(Path(a.reference), out)
+        gen_symbols(Path(a.reference), out)
+        gen_binding_argtypes(binding, out)
+        gen_abi_traces(binding, Path(a.reference), out)
     for f in sorted(out.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
