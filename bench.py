@@ -167,9 +167,22 @@ def gpu_uuid(dev: int):
 
 # ---------------------------------------------------------------- CPU baseline
 
-def cpu_reference_run(gates, n_target, seconds, max_gates=None):
-    """Time the reference OpenMP core gate by gate on the first gates of the circuit.
-    Returns (gb_per_s, gates_done, qubits, kind, threads)."""
+def _omp_set_threads(k):
+    """Thread count of the OpenMP team the reference core's kernels use (calls
+    from this thread); returns False where libgomp cannot be reached."""
+    import ctypes
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(k))
+        return True
+    except OSError:
+        return False
+
+
+def cpu_reference_run(gates, n_target, seconds, repeats=5):
+    """Time the reference OpenMP core gate by gate on the first gates of the
+    circuit: `repeats` samples with all host threads (the gate count per sample
+    sized to ~seconds/repeats) and `repeats` one-gate samples on one thread;
+    medians of each.  Returns a dict."""
     from oracle.oracle import Port, RefCore
     avail = 0
     try:
@@ -194,17 +207,31 @@ def cpu_reference_run(gates, n_target, seconds, max_gates=None):
         kind, threads = "port", 1
         apply1 = lambda q, U: port.apply_1q(st, n, q, U)  # noqa: E731
         apply2 = lambda a, b, U: port.apply_2q(st, n, a, b, U)  # noqa: E731
-    done = 0
-    t0 = time.perf_counter()
-    for qs, U in gates:
-        if max_gates is not None and done >= max_gates:
-            break
-        (apply1(qs[0], U) if len(qs) == 1 else apply2(qs[0], qs[1], U))
-        done += 1
-        if max_gates is None and time.perf_counter() - t0 > seconds:
-            break
-    dt = time.perf_counter() - t0
-    return done * pass_bytes(n) / dt / 1e9, done, n, kind, threads, dt
+    pos = [0]
+
+    def run(count):
+        t0 = time.perf_counter()
+        for _ in range(count):
+            qs, U = gates[pos[0] % len(gates)]
+            pos[0] += 1
+            (apply1(qs[0], U) if len(qs) == 1 else apply2(qs[0], qs[1], U))
+        return time.perf_counter() - t0
+
+    if kind == "reference":
+        _omp_set_threads(threads)
+    first = run(1)                                          # warm-up gate (first touch, thread start)
+    per = max(1, int((seconds / repeats) / max(first, 1e-3)))
+    rates = []
+    for _ in range(repeats):
+        rates.append(per * pass_bytes(n) / run(per) / 1e9)
+    out = {"gbs": statistics.median(rates), "n": n, "kind": kind, "threads": threads, "gates_per_sample": per,
+           "samples": repeats, "samples_gbs": [round(r, 2) for r in rates]}
+    if kind == "reference" and threads > 1 and _omp_set_threads(1):
+        one = [pass_bytes(n) / run(1) / 1e9 for _ in range(repeats)]
+        _omp_set_threads(threads)
+        out["one_thread_gbs"] = statistics.median(one)
+        out["one_thread_samples_gbs"] = [round(r, 2) for r in one]
+    return out
 
 
 def reference_arm(args, rank):
@@ -279,17 +306,25 @@ def adjoint_section(args, rank, world):
     import torch
     from invariantq_b200.gradients import adjoint_gradient_batch, adjoint_stats, parameter_shift_gradient
     from invariantq_b200.replicas import max_over_ranks, shard
+    import tempfile as _tf
+    from invariantq_b200.autotune import AdjointAutotuner, adjoint_settings
     jobs = gradient_jobs(args.adjoint_circuits, args.adjoint_sets)
     mine = shard(jobs, rank, world)
     grads = sum(P.shape[0] for _, _, P in mine)
     partials = sum(P.shape[0] * P.shape[1] for _, _, P in mine)
-    adjoint_gradient_batch(mine, args.adjoint_streams)            # warm-up (allocations, first plans)
-    times = []
-    for _ in range(max(args.adjoint_steps, 1)):
-        t0 = time.perf_counter()
-        out = adjoint_gradient_batch(mine, args.adjoint_streams)
-        times.append(time.perf_counter() - t0)
-    st = adjoint_stats()
+    # executor settings picked by the project's autotuner on every 8th circuit (not timed)
+    tuner = AdjointAutotuner(Path(_tf.mkdtemp()) / "autotune.json", stride=8)
+    t_tune = time.perf_counter()
+    choice = tuner.choose(mine)
+    tune_s = time.perf_counter() - t_tune
+    with adjoint_settings(choice):
+        adjoint_gradient_batch(mine, args.adjoint_streams)            # warm-up (allocations, first plans)
+        times = []
+        for _ in range(max(args.adjoint_steps, 1)):
+            t0 = time.perf_counter()
+            out = adjoint_gradient_batch(mine, args.adjoint_streams)
+            times.append(time.perf_counter() - t0)
+        st = adjoint_stats()
     t = max_over_ranks(float(np.median(times)), device=f"cuda:{int(os.environ.get('LOCAL_RANK', 0))}")
     # parameter-shift baseline on every k-th circuit of this rank (first parameter set)
     ps_t, ps_n, err = 0.0, 0, 0.0
@@ -316,6 +351,11 @@ def adjoint_section(args, rank, world):
                         "seconds": round(ps_t, 2)},
         "speedup_vs_param_shift": round((grads / t) / ps_rate, 1),
         "max_abs_diff_vs_param_shift": err,
+        "settings": {"choice_id": choice["choice_id"], "tile_bits": choice["tile_bits"],
+                     "chunk_bits": choice["chunk_bits"], "budget": choice["budget"],
+                     "ctas_per_sm": choice["schedule"][0], "nbuf": choice["schedule"][1],
+                     "autotune": {"candidates_ms": choice["candidates_ms"], "measured": tuner.measured,
+                                  "sample_circuits": choice["sample_jobs"], "tune_s": round(tune_s, 1)}},
     }
 
 
@@ -386,46 +426,53 @@ def brickwall20_section(args):
 
 def fusion_sweep_section(args, sv, n, stream):
     """The 30-qubit circuit through GateFusionPass at k = 2..5: blocks, tile
-    passes after planning, passes/s and GB/s (2 x 16 B x 2^n per pass)."""
+    passes after planning, passes/s and GB/s (2 x 16 B x 2^n per pass), with
+    each block applied as the driver does ('cost': its dense matrix, or its
+    original gates where those need less FP64 work per amplitude) and, beside
+    it, every block as its dense 2^k x 2^k matrix ('dense')."""
     from invariantq_b200.circuits import brickwall
     from invariantq_b200.fusion import GateFusionPass
-    from invariantq_b200.simulator import apply_gate_matrix
+    from invariantq_b200.simulator import apply_fused_op, apply_gate_matrix
     c = brickwall(n, args.depth, seed=args.seed)
     out = {}
     for k in (2, 3, 4, 5):
         f = GateFusionPass(k).run(c)
-        with sv.record() as rec:
-            for op in f.ops:
-                qs = [f.get_qubit_index(q) for q in op.qubits]
-                if type(op).__name__ == "FusedGateOp":
-                    sv.apply_fused(qs, op.fused_matrix)
-                else:
-                    apply_gate_matrix(sv, qs, op.matrix)
-        prog = rec.program
+        row = {"blocks": len(f.ops)}
+        for policy in ("cost", "dense"):
+            how = {"dense": 0, "originals": 0}
+            with sv.record() as rec:
+                for op in f.ops:
+                    qs = [f.get_qubit_index(q) for q in op.qubits]
+                    if type(op).__name__ == "FusedGateOp":
+                        how[apply_fused_op(sv, f, op, policy)] += 1
+                    else:
+                        apply_gate_matrix(sv, qs, op.matrix)
+            prog = rec.program
 
-        def step():
-            sv.reset()
-            prog.run(sv)
+            def step():
+                sv.reset()
+                prog.run(sv)
 
-        step()
-        sv.sync()
-        ms = cuda_ms(stream, step)
-        sv.sync()
-        out[str(k)] = {"blocks": len(f.ops), "passes": prog.passes, "circuit_ms": round(ms, 2),
-                       "passes_per_s": round(prog.passes / (ms / 1e3), 2),
-                       "GBs": round(prog.passes * pass_bytes(n) / (ms / 1e3) / 1e9, 1)}
-        del prog
+            step()
+            sv.sync()
+            ms = cuda_ms(stream, step)
+            sv.sync()
+            row[policy] = {"fused_blocks_dense": how["dense"], "fused_blocks_as_original_gates": how["originals"],
+                           "passes": prog.passes, "circuit_ms": round(ms, 2),
+                           "passes_per_s": round(prog.passes / (ms / 1e3), 2),
+                           "GBs": round(prog.passes * pass_bytes(n) / (ms / 1e3) / 1e9, 1)}
+            del prog
+        out[str(k)] = row
     return out
 
 
-def fewer_passes_section(args, sv, n, gates, stream):
-    """The default 30-qubit circuit planned with 3 chunk qubits and budget 160
-    (the handle options for the fastest circuit): fewer, fuller passes, so a
-    shorter circuit at a lower bandwidth per pass.  Run last on the handle
-    (the options stay set)."""
+def plan_section(args, sv, n, gates, stream, opts, label):
+    """The 30-qubit circuit recorded with other handle options (`opts`),
+    timed on the device; its amplitudes' <Z_q> against the headline run's
+    (`ref_z`).  Options stay set on the handle, so run it after the headline."""
     from invariantq_b200.simulator import apply_gate_matrix
-    sv.set_option("chunk_bits", 3)
-    sv.set_option("budget", 160)
+    for k, v in opts.items():
+        sv.set_option(k, v)
     with sv.record() as rec:
         for qs, U in gates:
             apply_gate_matrix(sv, qs, U)
@@ -440,10 +487,33 @@ def fewer_passes_section(args, sv, n, gates, stream):
     ms = cuda_ms(stream, step)
     sv.sync()
     z = sv.expval_z_all()
-    return {"options": {"chunk_bits": 3, "budget": 160}, "passes": prog.passes, "circuit_ms": round(ms, 2),
+    return {"plan": label, "options": opts, "passes": prog.passes, "circuit_ms": round(ms, 2),
             "passes_per_s": round(prog.passes / (ms / 1e3), 2),
-            "GBs": round(prog.passes * pass_bytes(n) / (ms / 1e3) / 1e9, 1),
-            "z_finite": bool(np.all(np.isfinite(z)))}
+            "GBs_per_pass": round(prog.passes * pass_bytes(n) / (ms / 1e3) / 1e9, 1), "z": z}
+
+
+def autotune_section(args, sv, n, gates, stream, ref_z):
+    """The project's autotuner on the 30-qubit circuit (coordinate search over
+    tile bits, chunk bits, budget, register slots and CTAs per SM on the
+    circuit's first quarter; fusion width fixed at the runtime's own two-qubit
+    fusion), then the whole circuit timed with its choice."""
+    import tempfile as _tf
+    from invariantq_b200.autotune import Autotuner
+    from invariantq_b200.circuits import brickwall
+    c = brickwall(n, args.depth, seed=args.seed)
+    cache = Path(_tf.mkdtemp()) / "autotune.json"
+    tuner = Autotuner(cache, candidates={"k": (2,), "tile_bits": (11, 12), "chunk_bits": (3, 4, 5),
+                                         "budget": (120, 160, 200), "reg_slots": (4,), "ctas_per_sm": (2, 3, 4)})
+    t0 = time.perf_counter()
+    ch = tuner.choose(c)
+    tune_s = time.perf_counter() - t0
+    opts = {k: ch[k] for k in ("tile_bits", "chunk_bits", "budget", "reg_slots", "ctas_per_sm")}
+    run = plan_section(args, sv, n, gates, stream, opts, "autotuned")
+    z = run.pop("z")
+    run.update({"choice_id": ch["choice_id"], "candidates_measured": tuner.measured, "tune_s": round(tune_s, 1),
+                "probe_ms": ch["probe_ms"], "candidates_ms": ch["candidates_ms"],
+                "max_abs_z_diff_vs_headline": float(np.max(np.abs(z - ref_z)))})
+    return run
 
 
 def density_matrix_section(args):
@@ -575,7 +645,7 @@ def adjoint30_section(args):
     e32, g32 = adjoint_gradient_c64(a, h, th)
     t32 = time.perf_counter() - t0
     return {"workload": f"{n}q, {L} layers RY+RZ per qubit + CZ ring ({a.num_params} parameters), TFIM h=0.7, complex128; "
-                        "three state-sized buffers (psi and the 2^(n+1) psi/lambda array), no checkpoints",
+                        "state memory: one [psi | lambda] array of 2^(n+1) amplitudes (two state-sized buffers)",
             "gradient_s": round(t, 3), "energy": e, "passes": {"forward": int(st["forward_passes"]),
                                                               "backward": int(st["backward_passes"])},
             "achieved_gbs": round(st["bytes"] / t / 1e9, 1),
@@ -584,6 +654,41 @@ def adjoint30_section(args):
                           "grad_max_abs_err": float(np.max(np.abs(g32 - g))),
                           "grad_rel_err": float(np.max(np.abs(g32 - g)) / max(np.max(np.abs(g)), 1e-300)),
                           "states": "psi and lambda as complex64 (2 x 8 GiB), FP64 arithmetic and sums"}}
+
+
+def adjoint32_section(args):
+    """One 32-qubit adjoint gradient (4 layers of RY and RZ on every qubit plus
+    a CZ ring: 256 parameters; TFIM h = 0.7; complex128): the joint array
+    [psi | lambda] of 2^33 amplitudes (128 GiB) is the only state memory.
+    Checked against the parameter-shift rule on 2 parameters."""
+    import torch
+    from invariantq_b200.gradients import Ansatz, PauliHamiltonian, adjoint_gradient, adjoint_release, \
+        adjoint_stats, ansatz_energies, shifted_parameter_sets
+    free, _ = torch.cuda.mem_get_info()
+    if free < 140 * (1 << 30):
+        return {"skipped": f"needs ~130 GiB of free device memory ({free / 2**30:.0f} GiB free)"}
+    n, L = 32, 4
+    a, h = Ansatz.hardware_efficient(n, L), PauliHamiltonian.tfim(n, 0.7)
+    rng = np.random.default_rng(32)
+    th = rng.uniform(0, 2 * np.pi, a.num_params)
+    adjoint_gradient(a, h, th)                     # warm-up: planning, kernels, workspace
+    t0 = time.perf_counter()
+    e, g = adjoint_gradient(a, h, th)
+    t = time.perf_counter() - t0
+    st = adjoint_stats()
+    adjoint_release()
+    idx = rng.choice(a.num_params, 2, replace=False)
+    sets = shifted_parameter_sets(th)
+    rows = np.concatenate([[2 * j, 2 * j + 1] for j in idx])
+    es = ansatz_energies(a, h, sets[rows])
+    ps = 0.5 * (es[0::2] - es[1::2])
+    return {"workload": f"{n}q, {L} layers RY+RZ per qubit + CZ ring ({a.num_params} parameters), TFIM h=0.7, "
+                        "complex128; state memory: one [psi | lambda] array of 2^33 amplitudes (128 GiB)",
+            "gradient_s": round(t, 3), "energy": e,
+            "passes": {"forward": int(st["forward_passes"]), "backward": int(st["backward_passes"])},
+            "achieved_gbs": round(st["bytes"] / t / 1e9, 1),
+            "max_abs_diff_vs_param_shift": float(np.max(np.abs(ps - g[idx]))),
+            "checked_parameters": [int(i) for i in idx]}
 
 
 # ---------------------------------------------------------------- our arm
@@ -649,6 +754,7 @@ def our_arm(args, rank, world, local_rank):
     clk = clocks.stop() if clocks else None
     pass_ms = sv.profile_read()
     sv.set_option("profile", 0)
+    ref_z = sv.expval_z_all()          # <Z_q> after the last timed step (the whole circuit from |0...0>)
     ms = max_over_ranks(ms, device=f"cuda:{local_rank}")
 
     # e2e through the reference-facing C ABI (host matrices every step, <Z_i> read back)
@@ -675,20 +781,27 @@ def our_arm(args, rank, world, local_rank):
         e2e_ms = max_over_ranks(e2e_ms, device=f"cuda:{local_rank}")
         e2e = {"value": round(world * prog.passes * pass_bytes(n) / (e2e_ms / 1e3) / 1e9, 3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(8 * n + 4),
-               "ms_per_step": round(e2e_ms, 3), "specialised_passes_per_step": e2e_jit}
+               "ms_per_step": round(e2e_ms, 3), "specialised_passes_per_step": e2e_jit,
+               "max_abs_z_diff_vs_recorded_program": float(np.max(np.abs(z - ref_z)))}
         assert np.all(np.abs(z) <= 1.0 + 1e-9)
 
     adj = adjoint_section(args, rank, world) if not args.no_adjoint else None
     opts = {k: sv.get_option(k) for k in ("tile_bits", "chunk_bits", "budget", "max_stages", "nbuf", "reg_slots",
-                                          "jit")}
+                                          "ctas_per_sm", "jit")}
     configs = None
     if world == 1 and not args.no_configs:
         configs = {"fusion_sweep_30q": fusion_sweep_section(args, sv, n, stream)}
-        configs["fewer_passes_30q"] = fewer_passes_section(args, sv, n, gates, stream)
+        configs["autotune_30q"] = autotune_section(args, sv, n, gates, stream, ref_z)
+        other = plan_section(args, sv, n, gates, stream,
+                             {"tile_bits": 11, "chunk_bits": 5, "budget": 120, "ctas_per_sm": 4},
+                             "more passes: the interpreting kernel's tile shape (2^11, 5 chunk qubits), budget 120")
+        other["max_abs_z_diff_vs_headline"] = float(np.max(np.abs(other.pop("z") - ref_z)))
+        configs["plan_comparison_30q"] = other
         configs["brickwall_20q"] = brickwall20_section(args)
         sv.close()
         configs["density_matrix_14q"] = density_matrix_section(args)
         configs["adjoint_30q"] = adjoint30_section(args)
+        configs["adjoint_32q"] = adjoint32_section(args)
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
@@ -728,10 +841,17 @@ def our_arm(args, rank, world, local_rank):
     if configs is not None:
         out["configs"] = configs
     if world == 1 and not args.no_cpu_baseline:
-        gbs, done, nq, kind, threads, dt = cpu_reference_run(gates, n, args.cpu_seconds)
-        out["cpu_baseline"] = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": kind,
-                               "sample": f"first {done} gates of the {nq}-qubit depth-{args.depth} brick-wall, one "
-                                         f"pass per gate through the C ABI, {dt:.1f} s"}
+        cb = cpu_reference_run(gates, n, args.cpu_seconds)
+        out["cpu_baseline"] = {
+            "value": round(cb["gbs"], 3), "unit": UNIT, "cores": cb["threads"], "kind": cb["kind"],
+            "sample": f"median of {cb['samples']} samples of {cb['gates_per_sample']} consecutive gates of the "
+                      f"{cb['n']}-qubit depth-{args.depth} brick-wall (from its first gate), one pass per gate "
+                      f"through the C ABI, all {cb['threads']} host threads",
+            "samples_gbs": cb["samples_gbs"]}
+        if "one_thread_gbs" in cb:
+            out["cpu_baseline"]["one_core"] = {"value": round(cb["one_thread_gbs"], 3), "unit": UNIT, "cores": 1,
+                                               "sample": f"median of {cb['samples']} single-gate samples, 1 thread",
+                                               "samples_gbs": cb["one_thread_samples_gbs"]}
     print(json.dumps(out))
 
 

@@ -132,6 +132,14 @@ int iq_statevector_set_amplitudes(void* sv, const double* real_in, const double*
  * handle's stream (cudaStream_t) for ordering work against it. */
 void* iq_statevector_device_ptr(void* sv);
 void* iq_statevector_stream(void* sv);
+/* The half of the amplitudes whose index bit `bit` equals `value` (0 or 1), in
+ * increasing index order, copied to (pack) or from (unpack) a device buffer of
+ * 2^(n-1) complex128; queued gates are applied first and the copy has finished
+ * when the call returns.  The exchange step of a state vector sharded across
+ * GPUs by its top qubits (a global qubit swapped with a local one moves one
+ * such half to the partner rank).  No counterpart in the reference.  0 = ok. */
+int iq_statevector_pack_half(void* sv, size_t bit, int value, void* d_dst);
+int iq_statevector_unpack_half(void* sv, size_t bit, int value, const void* d_src);
 size_t iq_statevector_num_qubits(void* sv);
 
 /* Tuning / diagnostics for either handle kind ("inject_status" = code: set the
@@ -171,11 +179,15 @@ int iq_jit_wait(double timeout_s);
  * planned once into tile passes whose matrices and descriptors stay on the
  * device; program_run launches them on the handle's stream (any number of
  * times, on the handle's current amplitudes).  program_info: out[0] passes,
- * [1] operations, [2] matrix bytes, [3] planned arithmetic cost. */
+ * [1] operations, [2] matrix bytes, [3] planned arithmetic cost.
+ * program_pass_info: pass i's out[0] operations, [1] planned arithmetic cost
+ * (real multiply-adds per amplitude), [2] register stages, [3] tile bits M,
+ * [4] chunk bits c, [5] tiles; returns the count written, 0 past the end. */
 int   iq_handle_record_begin(void* h);
 void* iq_handle_record_end(void* h);
 int   iq_handle_program_run(void* h, void* prog);
 int   iq_program_info(void* prog, double* out, size_t n);
+int   iq_program_pass_info(void* prog, size_t i, double* out, size_t n);
 void  iq_program_free(void* prog);
 /* With option "profile" = 1 every tile pass is bracketed by CUDA events; this
  * returns up to max per-pass durations in ms (oldest first) and clears them. */

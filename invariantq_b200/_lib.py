@@ -96,6 +96,8 @@ SIGNATURES = {
     "iq_statevector_expval_pauli_sum": ([_v, _sz, c_dp, ctypes.c_char_p, c_dp, c_dp], _i),
     "iq_statevector_set_amplitudes": ([_v, c_dp, c_dp], _i),
     "iq_statevector_device_ptr": ([_v], _v),
+    "iq_statevector_pack_half": ([_v, _sz, _i, _v], _i),
+    "iq_statevector_unpack_half": ([_v, _sz, _i, _v], _i),
     "iq_statevector_stream": ([_v], _v),
     "iq_statevector_num_qubits": ([_v], _sz),
     "iq_handle_set_option": ([_v, ctypes.c_char_p, _d], _i),
@@ -106,6 +108,7 @@ SIGNATURES = {
     "iq_handle_record_end": ([_v], _v),
     "iq_handle_program_run": ([_v, _v], _i),
     "iq_program_info": ([_v, c_dp, _sz], _i),
+    "iq_program_pass_info": ([_v, _sz, c_dp, _sz], _i),
     "iq_program_free": ([_v], None),
     "iq_statevector_expval_z_all_noalloc": ([_v, _sz, _v, _v], _i),
     "iq_adjoint_gradient": ([_sz, _sz, c_ip, c_ip, c_ip, c_ip, _sz, c_dp, _sz, c_dp, ctypes.c_char_p, c_dp, c_dp],

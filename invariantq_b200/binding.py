@@ -71,6 +71,17 @@ class Program:
         self._lib.iq_program_info(ptr, _p(out), 4)
         self.passes, self.ops, self.matrix_bytes, self.planned_cost = int(out[0]), int(out[1]), out[2], out[3]
 
+    def pass_info(self) -> List[Dict[str, float]]:
+        """Per pass: operations, planned cost (real FMAs per amplitude),
+        register stages, tile bits, chunk bits, tiles."""
+        out, rows = np.zeros(6), []
+        keys = ("ops", "cost", "stages", "tile_bits", "chunk_bits", "tiles")
+        for i in range(self.passes):
+            if self._lib.iq_program_pass_info(self._ptr, i, _p(out), 6) != 6:
+                break
+            rows.append(dict(zip(keys, out.tolist())))
+        return rows
+
     def run(self, handle: "_Handle") -> None:
         if self._lib.iq_handle_program_run(handle._ptr, self._ptr) != 0:
             check(self._lib)
@@ -226,6 +237,19 @@ class NativeStateVector(_Handle):
         im = np.ascontiguousarray(a.imag)
         if self._lib.iq_statevector_set_amplitudes(self._ptr, _p(re), _p(im)) != 0:
             check(self._lib)
+
+    def pack_half(self, bit: int, value: int, d_dst: int) -> None:
+        """Copy the amplitudes with index bit `bit` == value (increasing index
+        order) to the device buffer at address d_dst (2^(n-1) complex128)."""
+        if self._lib.iq_statevector_pack_half(self._ptr, bit, value, ctypes.c_void_p(d_dst)) != 0:
+            check(self._lib)
+            raise RuntimeError("pack_half failed")
+
+    def unpack_half(self, bit: int, value: int, d_src: int) -> None:
+        """The reverse of pack_half: overwrite that half from the device buffer."""
+        if self._lib.iq_statevector_unpack_half(self._ptr, bit, value, ctypes.c_void_p(d_src)) != 0:
+            check(self._lib)
+            raise RuntimeError("unpack_half failed")
 
     def device_ptr(self) -> int:
         p = self._lib.iq_statevector_device_ptr(self._ptr)

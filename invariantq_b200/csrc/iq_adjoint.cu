@@ -69,15 +69,17 @@ struct Cfg {
   static Cfg from_env() {
     Cfg c;
     c.jit = env_int("IQ_ADJOINT_JIT", 1);
-    c.sp.M = env_int("IQ_TILE_BITS", 11);
-    c.sp.c = env_int("IQ_CHUNK_BITS", 5);
+    // defaults: the state-vector path's specialised-kernel settings (tiles of
+    // 2^12 amplitudes holding the 4 lowest index bits, budget 160, 3 CTAs per
+    // SM with one tile buffer each), measured best for the batched gradients too
+    c.sp.M = env_int("IQ_TILE_BITS", 12);
+    c.sp.c = env_int("IQ_CHUNK_BITS", 4);
     c.sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
-    // adjoint sweeps plan with the same budget as the state-vector default
-    c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 120.0));
+    c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 160.0));
     c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
-    c.tl.nbuf = env_int("IQ_NBUF", 3);
-    c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
+    c.tl.nbuf = env_int("IQ_NBUF", 1);
+    c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 3);
     c.tl.consumers = 128;
     c.fuse = env_int("IQ_FUSE", 1);
     return c;
@@ -256,7 +258,7 @@ void job_ops(const Cfg& cfg, const Circuit& c, const double* theta, bool backwar
   j.fw = cfg.fuse ? fuse_two_qubit_blocks(raw, j.fpool) : raw;
   if (!backward) return;
   raw.clear();
-  ansatz_backward(c.n, c.ops, theta, raw, j.bpool, j.grad_param);
+  ansatz_backward(c.n, c.ops, theta, raw, j.bpool, j.grad_param, c.n);   // select bit n: [psi | lambda]
   j.bw = cfg.fuse ? fuse_two_qubit_blocks(raw, j.bpool) : raw;
 }
 
@@ -338,7 +340,7 @@ struct Workspace {
   cudaEvent_t ev[2] = {nullptr, nullptr};
   Pending pend[2];
   int slot = 0;
-  std::map<std::pair<const Shape*, uint32_t>, std::vector<CUtensorMap>> tmaps;   // (shape, sets)
+  std::map<std::tuple<const Shape*, uint32_t, int>, std::vector<CUtensorMap>> tmaps;   // (shape, sets, gap)
   const Circuit* ham_of = nullptr;   // circuit whose Hamiltonian tables are on the device
 
   // The state arrays are sized up front for the batch's largest job; matrix,
@@ -403,9 +405,9 @@ struct Workspace {
   // Tensor maps of a shape's passes over `nsets` arrays at `base`.  Circuit
   // shapes live for the whole call and are cached; a job's private shape is
   // encoded into `scratch` (its address may be reused by a later shape).
-  const std::vector<CUtensorMap>* maps_for(const Shape& s, double2* base, uint32_t nsets, bool cache,
+  const std::vector<CUtensorMap>* maps_for(const Shape& s, double2* base, uint32_t nsets, int gap, bool cache,
                                            std::vector<CUtensorMap>& scratch, std::string& err) {
-    const auto key = std::make_pair(&s, nsets);
+    const auto key = std::make_tuple(&s, nsets, gap);
     if (cache) {
       auto it = tmaps.find(key);
       if (it != tmaps.end()) return &it->second;
@@ -415,6 +417,7 @@ struct Workspace {
     for (size_t i = 0; i < s.plans.size(); ++i) {
       PassDesc d = s.plans[i].desc;
       d.nsets = nsets;
+      d.gap = (uint8_t)gap;
       if (encode_pass_tmap(&v[i], base, s.nbits, d, emsg, sizeof(emsg)) != 0) {
         err = emsg;
         return nullptr;
@@ -442,15 +445,24 @@ int log2_u64(uint64_t x) {
 
 // Launch a shape's passes over `nsets` arrays of 2^nbits amplitudes at `state`
 // (set s's matrices at mats + s * mat_stride; gradient rows per set:
-// grad_stride).  Returns the tile-pass grid of the launches in *grid.
+// grad_stride).  set_stride: amplitudes from one array to the next (0: the
+// arrays lie end to end).  Tile passes take any stride of 2^(nbits + 1) as
+// the gap bit nbits (the arrays are the lower halves of [psi | lambda] blocks).
+// Returns the tile-pass grid of the launches in *grid.
 bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double2* state, uint32_t nsets,
                const double2* mats, uint32_t mat_stride, double* gpart, uint32_t grad_stride, unsigned* grid,
-               Stats& st, std::string& err) {
+               Stats& st, std::string& err, uint64_t set_stride = 0) {
   const uint64_t dim = 1ULL << s.nbits;
+  const uint64_t stride = set_stride ? set_stride : dim;
+  int gap = 0;
+  if (s.tiled && stride != dim) {
+    if (stride != 2 * dim) { err = "internal: tile passes over arrays spaced other than 2^(n+1) apart"; return false; }
+    gap = s.nbits;
+  }
   if (!s.tiled) {
     for (uint32_t k = 0; k < nsets; ++k)
       for (const SimpleOp& so : s.sops)
-        if (!cuda_ok(launch_simple_op(state + k * dim, s.nbits, so, mats + (size_t)k * mat_stride, w.stream),
+        if (!cuda_ok(launch_simple_op(state + k * stride, s.nbits, so, mats + (size_t)k * mat_stride, w.stream),
                      "gate kernel", err))
           return false;
     st.launches += s.sops.size() * nsets;
@@ -458,10 +470,11 @@ bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double
     return true;
   }
   std::vector<CUtensorMap> scratch;
-  const std::vector<CUtensorMap>* tm = w.maps_for(s, state, nsets, cached, scratch, err);
+  const std::vector<CUtensorMap>* tm = w.maps_for(s, state, nsets, gap, cached, scratch, err);
   if (!tm) return false;
   for (size_t i = 0; i < s.plans.size(); ++i) {
     PassDesc d = s.plans[i].desc;
+    d.gap = (uint8_t)gap;
     d.set_shift = (uint32_t)log2_u64(d.ntiles);
     d.ntiles *= nsets;
     d.nsets = nsets;
@@ -550,7 +563,7 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
   const double2* joint0 = w.joint.p;
   if (!w.mats.ensure(2 * per * S, err, "matrices", w.stream) ||
       !w.red.ensure((size_t)S * (kRedBlocks + 1), err, "reduction partials", w.stream) ||
-      !w.psi.ensure(dim * S, err, "the states", w.stream))
+      (!want_grad && !w.psi.ensure(dim * S, err, "the states", w.stream)))
     return false;
   const unsigned max_grid = (unsigned)w.num_sms * (unsigned)std::max(1, cfg.tl.ctas_per_sm);
   if (want_grad && (!w.joint.ensure(jdim * S, err, "the joint arrays", w.stream) ||
@@ -580,26 +593,30 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
                     (std::chrono::steady_clock::now() - t0) - (tw1 - tw))
                     .count();
 
-  // forward from |0> for every set
-  if (!cuda_ok(launch_set_basis_sets(w.psi.p, dim, (int)S, w.stream), "reset", err)) return false;
-  if (!run_shape(w, cfg, *fw, fw_cached, w.psi.p, S, dm, (uint32_t)nf, nullptr, 0, nullptr, st, err)) return false;
-  st.fw_passes += (fw->tiled ? fw->plans.size() : fw->sops.size()) * S;
   double* partials = w.red.p;
   double* energy_dev = w.red.p + (size_t)S * kRedBlocks;
   if (!want_grad) {
-    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, (int)S, 0, c.ham.groups, w.zmask.p, w.coef.p, nullptr,
+    // forward from |0> for every set on the state buffer, then the energies
+    if (!cuda_ok(launch_set_basis_sets(w.psi.p, dim, (int)S, w.stream), "reset", err)) return false;
+    if (!run_shape(w, cfg, *fw, fw_cached, w.psi.p, S, dm, (uint32_t)nf, nullptr, 0, nullptr, st, err)) return false;
+    st.fw_passes += (fw->tiled ? fw->plans.size() : fw->sops.size()) * S;
+    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, dim, c.n, (int)S, c.ham.groups, w.zmask.p, w.coef.p, nullptr, 0,
                                           partials, energy_dev, w.stream),
                  "energy kernel", err))
       return false;
     st.launches += 3;
+    st.bytes += S * 16ULL * dim;   // read psi
   } else {
-    if (nj > c.n + 1)
-      for (uint32_t j = 0; j < S; ++j)
-        if (!cuda_ok(cudaMemsetAsync(w.joint.p + j * jdim + 2 * dim, 0, (jdim - 2 * dim) * sizeof(double2), w.stream),
-                     "memset", err))
-          return false;
-    if (!cuda_ok(launch_hamiltonian_joint(w.psi.p, c.n, (int)S, jdim, c.ham.groups, w.zmask.p, w.coef.p, w.joint.p,
-                                          partials, energy_dev, w.stream),
+    // Each set's joint array is [psi | lambda] (select bit n; small circuits
+    // zero-padded to 2^7): the forward runs on the psi half in place, lambda =
+    // H psi is written to the other half, and the backward sweep runs on the
+    // whole array -- two state-sized buffers per set, no copy of psi.
+    if (!cuda_ok(launch_init_joint(w.joint.p, c.n, jdim, (int)S, w.stream), "reset", err)) return false;
+    if (!run_shape(w, cfg, *fw, fw_cached, w.joint.p, S, dm, (uint32_t)nf, nullptr, 0, nullptr, st, err, jdim))
+      return false;
+    st.fw_passes += (fw->tiled ? fw->plans.size() : fw->sops.size()) * S;
+    if (!cuda_ok(launch_hamiltonian_joint(w.joint.p, jdim, c.n, (int)S, c.ham.groups, w.zmask.p, w.coef.p,
+                                          w.joint.p + dim, jdim, partials, energy_dev, w.stream),
                  "Hamiltonian kernel", err))
       return false;
     unsigned grid = 0;
@@ -614,9 +631,9 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
     if (ngrads && grid == 0) { err = "internal: no gradient pass"; return false; }
     if (!cuda_ok(launch_row_sums(w.gpart.p, ngrads * (int)S, (int)grid, w.gsum.p, w.stream), "gradient sums", err))
       return false;
-    st.launches += 5;
+    st.launches += 6;
+    st.bytes += S * 32ULL * dim;   // read psi, write lambda
   }
-  st.bytes += S * (16ULL * dim + (want_grad ? 32ULL * dim : 0));   // read psi; write the joint arrays
   double* ho = w.hout[k].p;
   if (!cuda_ok(cudaMemcpyAsync(ho, energy_dev, S * sizeof(double), cudaMemcpyDeviceToHost, w.stream), "D2H", err) ||
       !cuda_ok(cudaMemcpyAsync(w.hstat[k].p, w.status.p, sizeof(int), cudaMemcpyDeviceToHost, w.stream), "D2H", err))
@@ -751,15 +768,15 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const Cfg cfg = Cfg::from_env();
-  // jobs: a circuit's parameter sets in groups whose states (psi: 16 B x 2^n,
-  // joint: 32 B x 2^n per set) fit the per-job budget; the energy-only path
-  // (the plain baseline) runs one set per job
+  // jobs: a circuit's parameter sets in groups whose joint arrays ([psi |
+  // lambda], 32 B x 2^n per set) fit the per-job budget; the energy-only path
+  // (the plain baseline) runs one set per job on a state buffer (16 B x 2^n)
   struct Job { Circuit* c; size_t set0, nsets; double cost; };
   std::vector<Job> jobs;
   const double job_bytes = env_double("IQ_ADJOINT_JOB_BYTES", 4.0 * (1ull << 30));
   Workspace::Bounds bd;
   for (auto& c : circs) {
-    const double per_set = 48.0 * std::ldexp(1.0, c->n);
+    const double per_set = 16.0 * std::ldexp(1.0, joint_bits(c->n));
     const size_t group = want_grad ? (size_t)std::max(1.0, std::floor(job_bytes / per_set)) : 1;
     // per set: at most 3 rotations per gate, each at most a dense 4x4 (16
     // elements) forward and one backward; at most 3 gradient terms per gate
@@ -767,7 +784,7 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
     for (size_t s0 = 0; s0 < c->nsets; s0 += group) {
       const size_t ns = std::min(group, c->nsets - s0);
       jobs.push_back({c.get(), s0, ns, (double)ns * std::ldexp((double)nops, c->n)});
-      bd.psi_amps = std::max<uint64_t>(bd.psi_amps, (uint64_t)ns << c->n);
+      if (!want_grad) bd.psi_amps = std::max<uint64_t>(bd.psi_amps, (uint64_t)ns << c->n);
       if (want_grad) bd.joint_amps = std::max<uint64_t>(bd.joint_amps, (uint64_t)ns << joint_bits(c->n));
       bd.mats = std::max(bd.mats, ns * 96 * nops);
       bd.sets = std::max(bd.sets, ns);

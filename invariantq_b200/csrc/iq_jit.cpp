@@ -233,11 +233,15 @@ void drain_at_exit() {
   S.idle.wait_for(lk, std::chrono::seconds(60), [&] { return S.busy == 0; });
 }
 
+// cache file of a source: keyed by the NVRTC version, the headers the source
+// includes (a change to the tile pipeline or the pass descriptor must not pick
+// up a cubin built from the old text) and the source itself
 std::string cubin_path(const std::string& dir, const std::string& src) {
   int maj = 0, min = 0;
   nvrtc().version(&maj, &min);
   char name[96];
-  const std::string tag = "nvrtc" + std::to_string(maj) + "." + std::to_string(min);
+  std::string tag = "nvrtc" + std::to_string(maj) + "." + std::to_string(min);
+  for (const char* h : kJitHeaderSources) tag += h;
   snprintf(name, sizeof(name), "/%016llx.cubin", (unsigned long long)fnv1a(tag + src));
   return dir + name;
 }

@@ -428,6 +428,27 @@ cudaError_t launch_set_basis_sets(double2* s, uint64_t dim, int nsets, cudaStrea
   return cudaGetLastError();
 }
 
+// The half of the 2^nbits amplitudes whose index bit `bit` equals `val`, in
+// increasing index order: dst[i] = s[insert val at bit `bit` into i] (pack), or
+// the reverse (unpack).  Runs of 2^bit consecutive amplitudes: coalesced for
+// bit >= 5.
+__global__ void half_copy_kernel(double2* __restrict__ s, int bit, int val, double2* __restrict__ buf, uint64_t half,
+                                 int unpack) {
+  const uint64_t lo = (1ULL << bit) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < half; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t j = ((i & ~lo) << 1) | ((uint64_t)val << bit) | (i & lo);
+    if (unpack) s[j] = buf[i];
+    else buf[i] = s[j];
+  }
+}
+
+cudaError_t launch_half_copy(double2* s, int nbits, int bit, int val, double2* buf, bool unpack, cudaStream_t st) {
+  if (bit < 0 || bit >= nbits) return cudaErrorInvalidValue;
+  const uint64_t half = 1ULL << (nbits - 1);
+  half_copy_kernel<<<grid_for(half, 256), 256, 0, st>>>(s, bit, val & 1, buf, half, unpack ? 1 : 0);
+  return cudaGetLastError();
+}
+
 __global__ void split_kernel(const double2* __restrict__ s, uint64_t n, double* __restrict__ re, double* __restrict__ im) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const double2 a = s[i];
@@ -585,12 +606,12 @@ cudaError_t launch_partial_trace(const double2* s, int nbits, const int* keep, i
 // psi[x ^ xmask_g]: Pauli strings sharing their X part share one gather.
 __global__ void row_sum_kernel(const double* __restrict__ in, int cols, double* __restrict__ out);
 
-// blockIdx.y = set: psi + set * dim, joint + set * jdim, partials + set * gridDim.x
-__global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64_t dim, HamTerms h,
+// blockIdx.y = set: psi + set * pstride, lam + set * lstride, partials + set * gridDim.x
+__global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64_t pstride, uint64_t dim, HamTerms h,
                                          const uint64_t* __restrict__ zmask, const double2* __restrict__ coef,
-                                         double2* __restrict__ joint, uint64_t jdim, double* __restrict__ partials) {
-  psi += blockIdx.y * dim;
-  if (joint) joint += blockIdx.y * jdim;
+                                         double2* __restrict__ lam_out, uint64_t lstride, double* __restrict__ partials) {
+  psi += blockIdx.y * pstride;
+  if (lam_out) lam_out += blockIdx.y * lstride;
   partials += (size_t)blockIdx.y * gridDim.x;
   double e = 0.0;
   for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
@@ -607,23 +628,37 @@ __global__ void hamiltonian_joint_kernel(const double2* __restrict__ psi, uint64
       }
       lam = cfma(lam, f, a);
     }
-    if (joint) {
-      joint[2 * x] = px;
-      joint[2 * x + 1] = lam;
-    }
+    if (lam_out) lam_out[x] = lam;
     e += px.x * lam.x + px.y * lam.y;
   }
   e = block_sum(e);
   if (threadIdx.x == 0) partials[blockIdx.x] = e;
 }
 
-cudaError_t launch_hamiltonian_joint(const double2* psi, int n, int nsets, uint64_t jdim, const HamTerms& h,
-                                     const uint64_t* zmask, const double2* coef, double2* joint, double* partials,
-                                     double* energy, cudaStream_t st) {
+cudaError_t launch_hamiltonian_joint(const double2* psi, uint64_t pstride, int n, int nsets, const HamTerms& h,
+                                     const uint64_t* zmask, const double2* coef, double2* lam, uint64_t lstride,
+                                     double* partials, double* energy, cudaStream_t st) {
   if (nsets < 1) nsets = 1;
-  hamiltonian_joint_kernel<<<dim3(kRedBlocks, nsets), kRedThreads, 0, st>>>(psi, 1ULL << n, h, zmask, coef, joint,
-                                                                            jdim, partials);
+  hamiltonian_joint_kernel<<<dim3(kRedBlocks, nsets), kRedThreads, 0, st>>>(psi, pstride, 1ULL << n, h, zmask, coef,
+                                                                            lam, lstride, partials);
   row_sum_kernel<<<nsets, 256, 0, st>>>(partials, kRedBlocks, energy);
+  return cudaGetLastError();
+}
+
+// nsets joint arrays of jdim amplitudes end to end: psi half [0, dim) set to
+// e_0, everything above 2 * dim (zero padding of small circuits) to zero; the
+// lambda half [dim, 2 * dim) is left for the Hamiltonian kernel
+__global__ void init_joint_kernel(double2* __restrict__ s, uint64_t dim, uint64_t jdim, uint64_t total) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t l = i & (jdim - 1);
+    if (l < dim) s[i] = make_double2(l == 0 ? 1.0 : 0.0, 0.0);
+    else if (l >= 2 * dim) s[i] = make_double2(0.0, 0.0);
+  }
+}
+
+cudaError_t launch_init_joint(double2* s, int n, uint64_t jdim, int nsets, cudaStream_t st) {
+  const uint64_t total = jdim * (uint64_t)(nsets < 1 ? 1 : nsets);
+  init_joint_kernel<<<grid_for(total, 256), 256, 0, st>>>(s, 1ULL << n, jdim, total);
   return cudaGetLastError();
 }
 

@@ -71,6 +71,9 @@ cudaError_t launch_set_basis(double2* s, uint64_t dim, cudaStream_t st);   // s 
 // nsets arrays of dim amplitudes (dim a power of two) laid end to end, each set to e_0
 cudaError_t launch_set_basis_sets(double2* s, uint64_t dim, int nsets, cudaStream_t st);
 cudaError_t launch_split(const double2* s, uint64_t count, double* re, double* im, cudaStream_t st);
+// Copy the half of the 2^nbits amplitudes with index bit `bit` == val to buf
+// (unpack = false) or back from buf (unpack = true), in increasing index order.
+cudaError_t launch_half_copy(double2* s, int nbits, int bit, int val, double2* buf, bool unpack, cudaStream_t st);
 cudaError_t launch_probs(const double2* s, uint64_t count, double* p, cudaStream_t st);
 
 // ---- sampling ----
@@ -93,12 +96,15 @@ struct HamTerms {
   uint64_t xmask[kMaxHamGroups];
   int first[kMaxHamGroups + 1];
 };
-// For each of nsets states psi_s = psi + s * 2^n: joint_s[2x] = psi_s[x],
-// joint_s[2x+1] = (H psi_s)[x] with joint_s = joint + s * jdim (when joint is
-// not null), and energy[s] = Re <psi_s|H|psi_s>.  partials: nsets * kRedBlocks.
-cudaError_t launch_hamiltonian_joint(const double2* psi, int n, int nsets, uint64_t jdim, const HamTerms& h,
-                                     const uint64_t* zmask, const double2* coef, double2* joint, double* partials,
-                                     double* energy, cudaStream_t st);
+// For each of nsets states psi_s = psi + s * pstride (2^n amplitudes):
+// lambda_s = H psi_s written to lam + s * lstride (when lam is not null), and
+// energy[s] = Re <psi_s|H|psi_s>.  partials: nsets * kRedBlocks.
+cudaError_t launch_hamiltonian_joint(const double2* psi, uint64_t pstride, int n, int nsets, const HamTerms& h,
+                                     const uint64_t* zmask, const double2* coef, double2* lam, uint64_t lstride,
+                                     double* partials, double* energy, cudaStream_t st);
+// nsets joint arrays [psi | lambda | zero padding] of jdim amplitudes end to
+// end: psi halves (2^n amplitudes) set to e_0, padding above 2^(n+1) zeroed.
+cudaError_t launch_init_joint(double2* s, int n, uint64_t jdim, int nsets, cudaStream_t st);
 cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st);
 
 // Eigenvalues (ascending) of the reduced state on the kept qubits keep[0..k) of

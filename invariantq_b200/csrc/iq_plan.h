@@ -106,7 +106,12 @@ struct StageDesc {       // 28 bytes
 
 struct PassDesc {
   uint8_t M, c, R, nstages;
-  uint8_t nH, nbox, pad0, pad1;
+  uint8_t nH, nbox;
+  // gap != 0: tile addresses carry a zero at address bit `gap` (above every
+  // bit the pass touches), so the pass runs over the lower half of each
+  // 2^(gap + 1)-amplitude block -- e.g. the psi half of a [psi | lambda] array.
+  uint8_t gap;
+  uint8_t pad1;
   uint8_t H[kMaxTileBits + 3];   // physical bit of tile-local bit c + i (ascending)
   uint64_t ntiles;
   uint32_t nops, pad2;
@@ -177,6 +182,7 @@ IQ_HD uint64_t tile_base(uint64_t t, const PassDesc& P) {
     const int h = P.H[i];
     x = ((x >> h) << (h + 1)) | (x & ((1ULL << h) - 1));
   }
+  if (P.gap) x = ((x >> P.gap) << (P.gap + 1)) | (x & ((1ULL << P.gap) - 1));
   return x;
 }
 
@@ -203,6 +209,7 @@ IQ_HD uint32_t swz(uint32_t j) { return j ^ ((j >> 3) & 7u); }
 // values of H0 and H1, so one copy moves 2^(c + nbox) amplitudes; the other
 // tile bits are enumerated by issues.
 IQ_HD void pass_tmap_layout(const PassDesc& d, int nbits, uint64_t gd[5], uint64_t gs[4], uint32_t box[5]) {
+  if (d.gap) nbits = d.gap + 1;   // the map covers the whole 2^(gap + 1) block of each array
   const int c = d.c;
   const uint64_t E = 16;
   const uint64_t top = (1ull << nbits) * E;
@@ -261,14 +268,17 @@ struct TileCoordMap {
   int n3;                 // dim 3 (nbox 2): (t >> n1) & ((1 << n3) - 1)
   int shhi;               // top-dimension bits start at t >> shhi
   int ngap;
-  uint8_t gap[kMaxTileBits];   // ascending zero positions in the top coordinate
+  uint8_t gap[kMaxTileBits + 1];   // ascending zero positions in the top coordinate
+  int gap1;               // nbox 0: zero position in dim 1 (-1: none)
 };
 
 IQ_HD void tile_coord_map(const PassDesc& P, TileCoordMap& m) {
   m.nbox = P.nbox;
   m.ngap = 0;
+  m.gap1 = -1;
   if (P.nbox == 0) {       // the chunk alone: dim 1 = A >> 3 = t << (c - 3)
     m.n1 = 31; m.sh1 = P.c - 3; m.n3 = 0; m.shhi = 31;
+    if (P.gap) m.gap1 = P.gap - 3;
     return;
   }
   const int h0 = P.H[0];
@@ -279,14 +289,21 @@ IQ_HD void tile_coord_map(const PassDesc& P, TileCoordMap& m) {
   m.shhi = m.n1 + m.n3;
   m.gap[m.ngap++] = 0;                          // bit `lo` itself is a tile bit
   for (int i = P.nbox; i < P.nH; ++i) m.gap[m.ngap++] = (uint8_t)(P.H[i] - lo);
+  if (P.gap) m.gap[m.ngap++] = (uint8_t)(P.gap - lo);   // above every tile bit: last
 }
 
 IQ_HD void tile_coords(uint32_t t, const TileCoordMap& m, int& c1, int& c2, int& c3, int& c4) {
   c1 = (int)((m.n1 >= 31 ? t : (t & ((1u << m.n1) - 1u))) << m.sh1);
   c2 = c3 = c4 = 0;
-  if (m.nbox == 0) return;
+  if (m.nbox == 0) {
+    if (m.gap1 >= 0) {
+      const uint32_t u = (uint32_t)c1;
+      c1 = (int)(((u >> m.gap1) << (m.gap1 + 1)) | (u & ((1u << m.gap1) - 1u)));
+    }
+    return;
+  }
   uint32_t x = m.shhi >= 32 ? 0u : (t >> m.shhi);
-  for (int i = 0; i < kMaxTileBits; ++i)
+  for (int i = 0; i < kMaxTileBits + 1; ++i)
     if (i < m.ngap) {
       const int g = m.gap[i];
       x = ((x >> g) << (g + 1)) | (x & ((1u << g) - 1u));

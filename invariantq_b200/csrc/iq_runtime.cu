@@ -216,21 +216,29 @@ struct Engine {
   int plan_style = 0;  // 0: by the jit setting; 1: as for the interpreting kernel; 2: as for specialised kernels
   int jit_threads = 0; // CTA size of specialised kernels (0: by register slots; 128 or 256)
   // settings given explicitly (option or environment); the others take the
-  // defaults of the plan style: specialised kernels run 4 CTAs per SM with one
-  // tile buffer each (measured best on the 30-qubit brick-wall)
-  bool set_c = false, set_budget = false, set_nbuf = false, set_ctas = false;
+  // defaults of the plan style.  Specialised kernels: tiles of 2^12 amplitudes
+  // holding the 4 lowest qubits, a budget of 160 FMAs per amplitude per pass,
+  // 3 CTAs per SM with one tile buffer each (the fastest 30-qubit brick-wall
+  // measured: 78 passes, ~627 ms, against 110 passes and ~776 ms with the
+  // interpreting kernel's 11 / 5 / 120 / 4 CTAs).  Interpreting kernel: tiles of
+  // 2^11 holding 5, budget 120, 2 CTAs per SM with three buffers.
+  bool set_M = false, set_c = false, set_budget = false, set_nbuf = false, set_ctas = false;
 
   bool spec_style() const {
     return plan_style == 2 || (plan_style == 0 && jit && (jit >= 2 || nbits >= kJitMinBits) && !eager && nbits >= 7);
   }
   SchedParams plan_params(bool spec) const {
     SchedParams p = sp;
-    (void)spec;
+    if (spec) {
+      if (!set_M) p.M = 12;
+      if (!set_c) p.c = 4;
+      if (!set_budget) p.budget = 160.0;
+    }
     return p;
   }
   TileLaunch launch_params(bool spec) const {
     TileLaunch t = tl;
-    if (spec && !set_ctas) t.ctas_per_sm = 4;
+    if (spec && !set_ctas) t.ctas_per_sm = 3;
     if (spec && !set_nbuf) t.nbuf = 1;
     return t;
   }
@@ -284,6 +292,7 @@ struct Engine {
     sp.budget = env_double("IQ_PASS_BUDGET", 120.0);
     tl.nbuf = env_int("IQ_NBUF", 3);
     tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 2);
+    set_M = getenv("IQ_TILE_BITS") != nullptr;
     set_c = getenv("IQ_CHUNK_BITS") != nullptr;
     set_budget = getenv("IQ_PASS_BUDGET") != nullptr;
     set_nbuf = getenv("IQ_NBUF") != nullptr;
@@ -959,11 +968,18 @@ double iq_statevector_entropy(void* sv, const size_t* qubits, size_t num_subsys_
       if (!in[q]) keep.push_back(q);
   }
   const int kk = (int)keep.size();
-  if (kk > 10) {
-    set_error(E_UNSUPPORTED, "entropy: the smaller side has %d qubits; at most 10 are supported", kk);
+  if (kk > reduced_spectrum_max_bits()) {
+    set_error(E_UNSUPPORTED, "entropy: the smaller side has %d qubits; at most %d are supported", kk,
+              reduced_spectrum_max_bits());
     return kNaN;
   }
   if (!e->sync()) return kNaN;
+  if (kk >= 7) {
+    // reduced state, tridiagonalisation and eigenvalues on the device (iq_entropy.cu)
+    std::vector<double> w;
+    if (!cuda_ok(reduced_spectrum(e->d_state, n, keep.data(), kk, w, e->stream), "reduced spectrum")) return kNaN;
+    return entropy_from(w);
+  }
   const size_t kd = (size_t)1 << kk;
   double2* d_rho = nullptr;
   if (!cuda_ok(cudaMallocAsync(&d_rho, kd * kd * sizeof(double2), e->stream), "cudaMallocAsync")) return kNaN;
@@ -1117,6 +1133,31 @@ int iq_statevector_set_amplitudes(void* sv, const double* real_in, const double*
   return cuda_ok(cudaStreamSynchronize(e->stream), "sync") ? 0 : -1;
 }
 
+static int half_copy(void* sv, size_t bit, int value, void* d_buf, bool unpack) {
+  Engine* e = as_engine(sv, 0);
+  if (!e || !d_buf) return -1;
+  if (bit >= (size_t)e->nbits || (value != 0 && value != 1)) {
+    set_error(E_ARG, "%s_half: bit %zu / value %d out of range for %d qubits", unpack ? "unpack" : "pack", bit, value,
+              e->nbits);
+    return -1;
+  }
+  if (!e->flush()) return -1;
+  ++g_launches;
+  ++e->st_launches;
+  if (!cuda_ok(launch_half_copy(e->d_state, e->nbits, (int)bit, value, static_cast<double2*>(d_buf), unpack, e->stream),
+               "half copy"))
+    return -1;
+  return cuda_ok(cudaStreamSynchronize(e->stream), "sync") ? 0 : -1;
+}
+
+int iq_statevector_pack_half(void* sv, size_t bit, int value, void* d_dst) {
+  return half_copy(sv, bit, value, d_dst, false);
+}
+
+int iq_statevector_unpack_half(void* sv, size_t bit, int value, const void* d_src) {
+  return half_copy(sv, bit, value, const_cast<void*>(d_src), true);
+}
+
 void* iq_statevector_device_ptr(void* sv) {
   Engine* e = as_engine(sv, 0);
   if (!e) return nullptr;
@@ -1139,7 +1180,7 @@ int iq_handle_set_option(void* h, const char* key, double v) {
   if (!e || !key) return -1;
   if (!e->flush()) return -1;
   const int iv = (int)v;
-  if (!strcmp(key, "tile_bits")) { if (iv < 7 || iv > kMaxTileBits) return -1; e->sp.M = iv; }
+  if (!strcmp(key, "tile_bits")) { if (iv < 7 || iv > kMaxTileBits) return -1; e->sp.M = iv; e->set_M = true; }
   else if (!strcmp(key, "chunk_bits")) { if (iv < 3 || iv > 7) return -1; e->sp.c = iv; e->set_c = true; }
   else if (!strcmp(key, "max_stages")) { if (iv < 1 || iv > kMaxStages) return -1; e->sp.max_stages = iv; }
   else if (!strcmp(key, "budget")) { if (v <= 0) return -1; e->sp.budget = v; e->set_budget = true; }
@@ -1168,9 +1209,9 @@ int iq_handle_set_option(void* h, const char* key, double v) {
 double iq_handle_get_option(void* h, const char* key) {
   Engine* e = static_cast<Engine*>(h);
   if (!e || !key) return kNaN;
-  if (!strcmp(key, "tile_bits")) return e->sp.M;
   // the values the handle's next plan uses (its plan style's defaults where not set)
   const bool spec = e->spec_style();
+  if (!strcmp(key, "tile_bits")) return e->plan_params(spec).M;
   if (!strcmp(key, "chunk_bits")) return e->plan_params(spec).c;
   if (!strcmp(key, "max_stages")) return e->sp.max_stages;
   if (!strcmp(key, "budget")) return e->plan_params(spec).budget;
@@ -1263,6 +1304,17 @@ int iq_program_info(void* prog, double* out, size_t n) {
                        (double)pg->pool_elems * sizeof(double2), planned_cost};
   const size_t m = std::min<size_t>(n, 4);
   for (size_t i = 0; i < m; ++i) out[i] = v[i];
+  return (int)m;
+}
+
+int iq_program_pass_info(void* prog, size_t i, double* out, size_t n) {
+  auto* pg = static_cast<Engine::Program*>(prog);
+  if (!pg || !out || !pg->tiled || i >= pg->plans.size()) return 0;
+  const PassPlan& p = pg->plans[i];
+  const double v[6] = {(double)p.desc.nops, p.cost, (double)p.desc.nstages, (double)p.desc.M, (double)p.desc.c,
+                       (double)p.desc.ntiles};
+  const size_t m = std::min<size_t>(n, 6);
+  for (size_t k = 0; k < m; ++k) out[k] = v[k];
   return (int)m;
 }
 

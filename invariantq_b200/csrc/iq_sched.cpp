@@ -329,11 +329,18 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 
   const uint64_t lowmask = (c >= 64) ? ~0ULL : ((1ULL << c) - 1);
   const uint64_t allmask = (nb >= 64) ? ~0ULL : ((1ULL << nb) - 1);
+  // the psi / lambda select bit of adjoint steps is local in every pass (as
+  // the chunk bits are): otherwise passes widened by the fixed gates first
+  // would leave it out and the steps could not join them
+  uint64_t select_mask = 0;
+  for (int i = 0; i < nops; ++i)
+    if (ops[i].grad) select_mask |= 1ULL << ops[i].q[0];
+  select_mask &= ~lowmask;
   int scheduled = 0;
   while (scheduled < nops) {
     if (ready.empty()) { err = "scheduler found no ready operation"; return -1; }
-    uint64_t local = whole ? allmask : lowmask;
-    int free_slots = whole ? 0 : (M - c);
+    uint64_t local = whole ? allmask : (lowmask | select_mask);
+    int free_slots = whole ? 0 : (M - c - __builtin_popcountll(select_mask));
     PassBuilder pb(p, c);
     std::vector<int> taken;
     double cost = 0.0;

@@ -13,9 +13,11 @@ Differences from the reference, each on purpose:
 * two-qubit noise-model entries (4x4 Kraus operators) use
   ``apply_2q_kraus``, which the reference driver calls but never defines
   (density_matrix.py:46-47);
-* the half-cut entanglement entropy is computed on the GPU when the smaller
-  side has at most 10 qubits and reported as ``None`` beyond that (the
-  reference's O(2^1.5n) CPU routine dominates its run time from 18 qubits on).
+* the half-cut entanglement entropy is computed on the GPU (reduced state,
+  tridiagonalisation and eigenvalues on the device) when the smaller side has
+  at most 13 qubits, i.e. up to 27 qubits, and reported as ``None`` beyond
+  that (the reference's O(2^1.5n) CPU routine dominates its run time from 18
+  qubits on).
 """
 from __future__ import annotations
 
@@ -88,13 +90,62 @@ def apply_gate_matrix(sv: NativeStateVector, qubits: List[int], matrix: np.ndarr
         sv.apply_fused(list(reversed(qubits)), matrix)
 
 
+def _is_monomial(m: np.ndarray) -> bool:
+    nz = np.abs(m) > 0.0
+    return bool((nz.sum(0) == 1).all() and (nz.sum(1) == 1).all())
+
+
+def matrix_cost(m: np.ndarray) -> float:
+    """Real FMAs per amplitude the tile planner spends on a k-qubit matrix: a
+    monomial one (a permutation with phases: X, CX, CZ, SWAP, S, T, RZ ...) at
+    most one complex scaling (1); a dense one-qubit gate 4 (the planner applies
+    it as a normalised real rotation and a one-sided phase, carrying the rest to
+    the next gate on its qubit); a dense k >= 2 block 2^k complex products per
+    amplitude (4 * 2^k)."""
+    m = np.asarray(m)
+    if _is_monomial(m):
+        return 1.0
+    return 4.0 if m.shape[0] == 2 else 4.0 * m.shape[0]
+
+
+def fused_block_choice(op) -> str:
+    """'originals' when applying a FusedGateOp's original gates costs no more
+    FP64 work per amplitude than its dense 2^k x 2^k block (the tile planner
+    groups them into the same passes either way), else 'dense'."""
+    originals = getattr(op, "original_ops", None) or []
+    if not originals:
+        return "dense"
+    dense = matrix_cost(op.fused_matrix)
+    split = sum(matrix_cost(o.matrix) for o in originals)
+    return "originals" if split <= dense else "dense"
+
+
+def apply_fused_op(sv: NativeStateVector, circuit, op, policy: str = "cost") -> str:
+    """Apply a FusedGateOp: its dense block through iq_statevector_apply_fused
+    (policy 'dense'), or, with policy 'cost', its original gates when they are
+    cheaper than the dense block (fused_block_choice).  Returns what was applied."""
+    how = fused_block_choice(op) if policy == "cost" else "dense"
+    if how == "originals":
+        for o in op.original_ops:
+            apply_gate_matrix(sv, [circuit.get_qubit_index(q) for q in o.qubits], np.asarray(o.matrix, np.complex128))
+    else:
+        sv.apply_fused([circuit.get_qubit_index(q) for q in op.qubits], op.fused_matrix)
+    return how
+
+
 class StateVectorSimulator:
     """``autotune``: None / False (default settings), True (an
     ``autotune.Autotuner`` with its default cache) or an ``Autotuner``; the
     chosen fusion width and tile-pass settings are applied and their choice ID
-    is reported in ``metadata["autotune"]``."""
+    is reported in ``metadata["autotune"]``.  ``fused_policy``: how FusedGateOp
+    blocks are applied ('cost': dense block or original gates, whichever needs
+    less FP64 work; 'dense': always the block)."""
 
-    def __init__(self, max_memory_bytes: Optional[int] = None, entropy_max_side: int = 10, autotune=None):
+    def __init__(self, max_memory_bytes: Optional[int] = None, entropy_max_side: int = 13, autotune=None,
+                 fused_policy: str = "cost"):
+        if fused_policy not in ("cost", "dense"):
+            raise ValueError("fused_policy must be 'cost' or 'dense'")
+        self.fused_policy = fused_policy
         self.name = "statevector"
         self.max_memory_bytes = max_memory_bytes
         self.entropy_max_side = entropy_max_side
@@ -129,8 +180,10 @@ class StateVectorSimulator:
         try:
             sv = NativeStateVector(n)
             if tuned is not None:
-                for key in ("tile_bits", "budget", "reg_slots"):
-                    sv.set_option(key, tuned[key])
+                from .autotune import HANDLE_OPTIONS
+                for key in HANDLE_OPTIONS:
+                    if key in tuned:
+                        sv.set_option(key, tuned[key])
             sv.set_option("profile", 1)
             for op in circuit.ops:
                 if ctx is not None:
@@ -144,8 +197,7 @@ class StateVectorSimulator:
                         raise ValueError(f"Gate '{op.name}' is not a finite unitary matrix")
                     apply_gate_matrix(sv, qubits, m)
                 elif kind == "FusedGateOp":
-                    qubits = [circuit.get_qubit_index(q) for q in op.qubits]
-                    sv.apply_fused(qubits, op.fused_matrix)
+                    apply_fused_op(sv, circuit, op, self.fused_policy)
                 elif kind == "ResetOp":
                     sv.reset_qubit(circuit.get_qubit_index(op.qubit))
             if ctx is not None:
@@ -183,8 +235,8 @@ class StateVectorSimulator:
                       "achieved_GBps": (float(stats["bytes"]) / kernel_ms / 1e6) if kernel_ms > 0 else None,
                       "autotune": None if tuned is None else {
                           "choice_id": tuned["choice_id"], "cached": tuned["cached"], "k": tuned["k"],
-                          "tile_bits": tuned["tile_bits"], "budget": tuned["budget"],
-                          "reg_slots": tuned["reg_slots"]},
+                          **{k: tuned[k] for k in ("tile_bits", "chunk_bits", "budget", "reg_slots", "ctas_per_sm")
+                             if k in tuned}},
                       "provenance": {"requested_backend": self.name, "selected_backend": "statevector",
                                      "implementation": "dense_statevector", "native": True,
                                      "exact": not allow_non_unitary, "resource_limit_bytes": self.max_memory_bytes,

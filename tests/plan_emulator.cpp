@@ -34,6 +34,15 @@ struct Emu {
     uint32_t box[5];
     pass_tmap_layout(P, nbits, gd, gs, box);
     const uint64_t base = tile_base(t, P);
+    {   // the kernel's 32-bit tile-coordinate map gives the same first copy
+      TileCoordMap m;
+      tile_coord_map(P, m);
+      int a[4], b[4];
+      tile_coords((uint32_t)t, m, a[0], a[1], a[2], a[3]);
+      chunk_coords(base, P, b[0], b[1], b[2], b[3]);
+      for (int d = 0; d < 4; ++d)
+        if (a[d] != b[d]) { err = "tile coordinate map disagrees with the 64-bit tile address"; return false; }
+    }
     const int nissue = 1 << (P.nH - P.nbox);
     const uint32_t box_elems = 1u << (P.c + P.nbox);
     double* sd = reinterpret_cast<double*>(state);
@@ -214,8 +223,10 @@ struct Emu {
 };
 
 // plan `ops` (optionally fused) and run every pass on `state`
+// gap != 0: the operations act on the lower half (address bit `gap` = 0) of a
+// state of gap + 1 bits, through passes planned for `gap` bits (PassDesc::gap)
 int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stages, double budget, int fuse,
-             int* npasses, int* ops_per_pass, char* errbuf, int errlen) {
+             int* npasses, int* ops_per_pass, char* errbuf, int errlen, int gap = 0) {
   if (fuse) {
     std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(e.pool.data()),
                            reinterpret_cast<const cplx64*>(e.pool.data()) + e.pool.size());
@@ -223,7 +234,7 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
     e.pool.assign(reinterpret_cast<const cd*>(cp.data()), reinterpret_cast<const cd*>(cp.data()) + cp.size());
   }
   SchedParams p{};
-  p.nbits = e.nbits;
+  p.nbits = gap ? gap : e.nbits;
   p.M = M;
   p.c = c;
   p.R = R;
@@ -235,6 +246,7 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
     snprintf(errbuf, errlen, "plan: %s", err.c_str());
     return -1;
   }
+  for (PassPlan& pl : plans) pl.desc.gap = (uint8_t)gap;
   if (npasses) *npasses = (int)plans.size();
   std::vector<cplx64> packed;
   pack_pass_matrices(plans, reinterpret_cast<const cplx64*>(e.pool.data()), packed);
@@ -256,8 +268,13 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
       if (!e.copy_tile(P, t, tile, false, seen)) break;
     }
     if (e.err.empty())
-      for (size_t i = 0; i < seen.size(); ++i)
-        if (!seen[i]) { e.err = "amplitude not covered by a pass"; break; }
+      for (size_t i = 0; i < seen.size(); ++i) {
+        const bool in_pass = !gap || !((i >> gap) & 1);
+        if (seen[i] != (in_pass ? 1 : 0)) {
+          e.err = in_pass ? "amplitude not covered by a pass" : "amplitude outside the pass's half touched";
+          break;
+        }
+      }
     if (!e.err.empty()) {
       snprintf(errbuf, errlen, "pass %zu: %s", pi, e.err.c_str());
       return -1;
@@ -283,18 +300,23 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
     snprintf(errbuf, errlen, "%s", err.c_str());
     return -1;
   }
-  // forward
-  Emu f;
-  f.nbits = n;
+  // the joint array [psi | lambda] (select bit n; zero-padded high bits for
+  // small circuits); the forward runs on its psi half
+  const int nj = std::max(n + 1, 7);
+  std::vector<cd> joint((size_t)1 << nj, 0.0);
   std::vector<cd> psi((size_t)1 << n, 0.0);
   psi[0] = 1.0;
-  f.state = psi.data();
+  Emu f;
   std::vector<SchedOp> fw;
   std::vector<cplx64> pool;
   ansatz_forward(n, ops, params, fw, pool);
   f.pool.assign(reinterpret_cast<const cd*>(pool.data()), reinterpret_cast<const cd*>(pool.data()) + pool.size());
-  if (n >= 7) {
-    if (run_plan(f, fw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+  if (n >= 7) {   // passes planned for n bits with the select bit as their gap
+    joint[0] = 1.0;
+    f.nbits = n + 1;
+    f.state = joint.data();
+    if (run_plan(f, fw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen, n) < 0) return -1;
+    for (uint64_t x = 0; x < (1ULL << n); ++x) psi[x] = joint[x];
   } else {   // the runtime's one-operation kernel: dense matrix, LSB-first qubit list
     for (const SchedOp& o : fw) {
       const int d = 1 << o.k;
@@ -340,16 +362,15 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
   cd e = 0.0;
   for (uint64_t x = 0; x < dim; ++x) e += std::conj(psi[x]) * lam[x];
   *energy = e.real();
-  // backward on the joint array
+  // backward on the joint array: psi at [0, 2^n), lambda at [2^n, 2^(n+1))
   Emu b;
-  b.nbits = std::max(n + 1, 7);   // small circuits: zero-padded high bits the gates never touch
-  std::vector<cd> joint((size_t)1 << b.nbits, 0.0);
-  for (uint64_t x = 0; x < dim; ++x) { joint[2 * x] = psi[x]; joint[2 * x + 1] = lam[x]; }
+  b.nbits = nj;   // small circuits: zero-padded high bits the gates never touch
+  for (uint64_t x = 0; x < dim; ++x) { joint[x] = psi[x]; joint[dim + x] = lam[x]; }
   b.state = joint.data();
   std::vector<SchedOp> bw;
   std::vector<cplx64> bpool;
   std::vector<int> gp;
-  ansatz_backward(n, ops, params, bw, bpool, gp);
+  ansatz_backward(n, ops, params, bw, bpool, gp, n);
   b.pool.assign(reinterpret_cast<const cd*>(bpool.data()), reinterpret_cast<const cd*>(bpool.data()) + bpool.size());
   b.grads.assign(gp.size(), 0.0);
   if (run_plan(b, bw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
@@ -526,7 +547,7 @@ extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int*
     std::vector<cplx64> pool;
     std::vector<int> gp;
     if (pass == 0) ansatz_forward(n, ops, params, raw, pool);
-    else ansatz_backward(n, ops, params, raw, pool, gp);
+    else ansatz_backward(n, ops, params, raw, pool, gp, n);
     const std::vector<SchedOp> fused = fuse_two_qubit_blocks(raw, pool);
     SchedParams p{};
     p.nbits = pass == 0 ? n : n + 1;
