@@ -312,8 +312,11 @@ def adjoint_section(args, rank, world):
     mine = shard(jobs, rank, world)
     grads = sum(P.shape[0] for _, _, P in mine)
     partials = sum(P.shape[0] * P.shape[1] for _, _, P in mine)
-    # executor settings picked by the project's autotuner on every 8th circuit (not timed)
-    tuner = AdjointAutotuner(Path(_tf.mkdtemp()) / "autotune.json", stride=8)
+    # executor settings picked by the project's autotuner on every 16th circuit (not timed; each
+    # candidate compiles the kernels of its pass structures, so the search is kept short)
+    tuner = AdjointAutotuner(Path(_tf.mkdtemp()) / "autotune.json", stride=16, rounds=1,
+                             candidates={"tile_bits": (12,), "chunk_bits": (4, 5), "budget": (160, 200),
+                                         "schedule": ((3, 1), (2, 1))})
     t_tune = time.perf_counter()
     choice = tuner.choose(mine)
     tune_s = time.perf_counter() - t_tune
@@ -343,6 +346,7 @@ def adjoint_section(args, rank, world):
         "warmup": 1, "gradients": world * grads, "streams": int(st["streams"]),
         "passes": {"forward": int(st["forward_passes"]), "backward": int(st["backward_passes"])},
         "achieved_gbs": round(st["bytes"] / t / 1e9, 1), "host_prep_ms": round(st["host_ms"], 1),
+        "resident_sets": int(st.get("resident_sets", 0)),
         "workload": f"{args.adjoint_circuits} circuits n~U{{10..22}} (here {min(ns)}..{max(ns)}), L~U{{4..12}}, "
                     f"RY+RZ per qubit + CZ ring per layer, {args.adjoint_sets} parameter sets each, TFIM h=1.0, "
                     "complex128; timed through iq_adjoint_gradient_batch (host parameters in, host gradients out)",

@@ -138,6 +138,18 @@ void* iq_statevector_stream(void* sv);
  * when the call returns.  The exchange step of a state vector sharded across
  * GPUs by its top qubits (a global qubit swapped with a local one moves one
  * such half to the partner rank).  No counterpart in the reference.  0 = ok. */
+/* Measurement shots as sorted distinct outcomes and their counts, computed on
+ * the device (the same shots as iq_statevector_sample with this seed; the
+ * counts dictionary the reference's driver builds in Python,
+ * invariantq/simulator/statevector.py:105-114).  values_out and counts_out
+ * hold up to num_shots entries; *num_unique receives how many were written.
+ * At most 2^30 shots.  No counterpart in the reference ABI.  0 = ok. */
+int iq_statevector_sample_counts(void* sv, size_t num_shots, uint64_t seed, uint64_t* values_out,
+                                 uint64_t* counts_out, size_t* num_unique);
+/* `count` draws of std::uniform_real_distribution<double>(0, 1) over
+ * std::mt19937_64 seeded with `seed`, generated on the current device (the
+ * stream iq_statevector_sample uses).  0 = ok. */
+int iq_mt64_uniform(uint64_t seed, size_t count, double* out);
 int iq_statevector_pack_half(void* sv, size_t bit, int value, void* d_dst);
 int iq_statevector_unpack_half(void* sv, size_t bit, int value, const void* d_src);
 size_t iq_statevector_num_qubits(void* sv);
@@ -291,7 +303,11 @@ int iq_ansatz_energy(const iq_adjoint_circuit* circuit);
  * [1] forward passes, [2] backward passes, [3] kernel launches, [4] algorithmic
  * HBM bytes of the passes, [5] host preparation ms (summed over workers),
  * [6] wall ms, [7] streams used, [8] passes run by specialised kernels
- * (IQ_ADJOINT_JIT, default 1).  Returns the number of counters (9). */
+ * (IQ_ADJOINT_JIT, default 1), [9] parameter sets run by the persistent
+ * shared-memory executor (circuits of at most IQ_RESIDENT_MAX_QUBITS = 12
+ * qubits: one launch for all of them, fed from a device-side queue of
+ * (circuit, set) items and replayed from a captured CUDA graph).  Returns the
+ * number of counters (10). */
 int iq_adjoint_stats(double* out, size_t n);
 
 /* Failure-path check (no counterpart in the reference): one CTA waits, with

@@ -97,6 +97,8 @@ SIGNATURES = {
     "iq_statevector_set_amplitudes": ([_v, c_dp, c_dp], _i),
     "iq_statevector_device_ptr": ([_v], _v),
     "iq_statevector_pack_half": ([_v, _sz, _i, _v], _i),
+    "iq_statevector_sample_counts": ([_v, _sz, ctypes.c_uint64, c_u64p, c_u64p, c_szp], _i),
+    "iq_mt64_uniform": ([ctypes.c_uint64, _sz, c_dp], _i),
     "iq_statevector_unpack_half": ([_v, _sz, _i, _v], _i),
     "iq_statevector_stream": ([_v], _v),
     "iq_statevector_num_qubits": ([_v], _sz),

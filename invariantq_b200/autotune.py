@@ -218,7 +218,7 @@ class Autotuner:
 
 ADJOINT_SETTINGS = ("tile_bits", "chunk_bits", "budget", "schedule")
 # schedule = (resident CTAs per SM, tile buffers per CTA)
-ADJOINT_START = {"tile_bits": 12, "chunk_bits": 4, "budget": 160, "schedule": (3, 1)}
+ADJOINT_START = {"tile_bits": 12, "chunk_bits": 4, "budget": 200, "schedule": (3, 1)}
 ADJOINT_CANDIDATES = {"tile_bits": (11, 12), "chunk_bits": (3, 4, 5), "budget": (120, 160, 200),
                       "schedule": ((3, 1), (2, 1), (4, 1), (2, 3))}
 

@@ -184,6 +184,18 @@ class NativeStateVector(_Handle):
         check(self._lib)
         return out
 
+    def sample_counts(self, num_shots: int, seed: int = 42):
+        """(outcomes ascending, their counts) of the shots sample() draws with
+        this seed, sampled and counted on the device."""
+        vals = np.empty(max(num_shots, 1), dtype=np.uint64)
+        cnts = np.empty(max(num_shots, 1), dtype=np.uint64)
+        nu = ctypes.c_size_t()
+        if self._lib.iq_statevector_sample_counts(self._ptr, num_shots, seed, vals.ctypes.data_as(c_u64p),
+                                                  cnts.ctypes.data_as(c_u64p), ctypes.byref(nu)) != 0:
+            check(self._lib)
+            raise RuntimeError("sample_counts failed")
+        return vals[:nu.value].copy(), cnts[:nu.value].copy()
+
     def von_neumann_entropy(self, subsystem_qubits: List[int]) -> float:
         q = np.ascontiguousarray(subsystem_qubits, dtype=np.uint64)
         v = self._lib.iq_statevector_entropy(self._ptr, q.ctypes.data_as(c_szp), len(subsystem_qubits))
@@ -376,6 +388,17 @@ def selftest_bounded_wait(limit_ms: float = 20.0) -> tuple:
         check(lib)
         raise RuntimeError("iq_selftest_bounded_wait failed")
     return st, waited.value
+
+
+def mt64_uniform(seed: int, count: int) -> np.ndarray:
+    """`count` draws of uniform_real_distribution(0, 1) over mt19937_64(seed),
+    generated on the GPU (the numbers iq_statevector_sample uses)."""
+    lib = _lib.load()
+    out = np.empty(max(count, 1))
+    if lib.iq_mt64_uniform(int(seed), count, _p(out)) != 0:
+        check(lib)
+        raise RuntimeError("iq_mt64_uniform failed")
+    return out[:count].copy()
 
 
 def jit_info() -> dict:

@@ -26,9 +26,9 @@ INCLUDE = PKG.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", *ARCH]
 SOURCES = ["iq_tile_r3.cu", "iq_tile_r4.cu", "iq_tile_r5.cu", "iq_kernels.cu", "iq_runtime.cu", "iq_sched.cpp", "iq_noalloc.cu",
-           "iq_adjoint.cu", "iq_c64.cu", "iq_entropy.cu",
+           "iq_adjoint.cu", "iq_c64.cu", "iq_entropy.cu", "iq_resident.cu", "iq_sampling.cu",
            "iq_selftest.cu", "iq_jit.cpp", "iq_jitgen.cpp"]
-HEADERS = ["iq_kernels.h", "iq_plan.h", "iq_pipe.cuh", "iq_tile.cuh", "iq_c64.h", "iq_jit.h"]
+HEADERS = ["iq_kernels.h", "iq_plan.h", "iq_pipe.cuh", "iq_tile.cuh", "iq_c64.h", "iq_jit.h", "iq_resident.h"]
 # headers the run-time compiled pass kernels include, embedded into the library
 JIT_HEADERS = ["iq_plan.h", "iq_pipe.cuh"]
 JIT_INC = CSRC / "iq_jit_headers.inc"

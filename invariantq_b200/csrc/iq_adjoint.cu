@@ -44,6 +44,7 @@
 #include "iq_c64.h"
 #include "iq_jit.h"
 #include "iq_kernels.h"
+#include "iq_resident.h"
 #include "iq_plan.h"
 
 using namespace iqb;
@@ -66,17 +67,21 @@ struct Cfg {
   TileLaunch tl{};
   int fuse = 1;
   int jit = 1;   // specialised kernels (iq_jit.cpp) for the forward and backward passes
+  // complex64 states: every pass a specialised kernel that widens the loaded
+  // amplitudes to FP64 and rounds once on store (jit_launch_narrow)
+  bool c64 = false;
   static Cfg from_env() {
     Cfg c;
     c.jit = env_int("IQ_ADJOINT_JIT", 1);
-    // defaults: the state-vector path's specialised-kernel settings (tiles of
-    // 2^12 amplitudes holding the 4 lowest index bits, budget 160, 3 CTAs per
-    // SM with one tile buffer each), measured best for the batched gradients too
+    // defaults: the state-vector path's specialised-kernel tile shape (2^12
+    // amplitudes holding the 4 lowest index bits, 3 CTAs per SM with one tile
+    // buffer each) and a budget of 200 (the adjoint autotuner's choice for the
+    // batched-gradient workload)
     c.sp.M = env_int("IQ_TILE_BITS", 12);
     c.sp.c = env_int("IQ_CHUNK_BITS", 4);
     c.sp.R = std::min(5, std::max(3, env_int("IQ_SLOTS", 4)));
     c.sp.max_stages = env_int("IQ_MAX_STAGES", 8);
-    c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 160.0));
+    c.sp.budget = env_double("IQ_ADJOINT_BUDGET", env_double("IQ_PASS_BUDGET", 200.0));
     c.sp.grad_cost = env_double("IQ_GRAD_COST", 6.0);
     c.tl.nbuf = env_int("IQ_NBUF", 1);
     c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 3);
@@ -217,11 +222,19 @@ bool make_shape(const Cfg& cfg, int nbits, const std::vector<SchedOp>& fused, si
       s.grid = g;
     }
   }
-  if (cfg.jit) {   // kernels specialised to the passes (shared by every circuit with the same pass structure)
+  if (cfg.jit || cfg.c64) {   // kernels specialised to the passes (shared by every circuit with the same pass structure)
     std::vector<const PassDesc*> ds;
     for (const PassPlan& pl : s.plans) ds.push_back(&pl.desc);
     std::string jerr;
-    if (!jit_prepare(ds, s.jit, jerr, cfg.tl.ctas_per_sm, 0, true)) s.jit.clear();
+    if (!jit_prepare(ds, s.jit, jerr, cfg.tl.ctas_per_sm, 0, true, cfg.c64)) s.jit.clear();
+    if (cfg.c64) {
+      bool all = s.jit.size() == s.plans.size();
+      for (const JitKernel* k : s.jit) all = all && k;
+      if (!all) {
+        err = "complex64 passes need run-time compiled kernels: " + (jerr.empty() ? std::string("kernel cache full") : jerr);
+        return false;
+      }
+    }
   }
   return true;
 }
@@ -454,6 +467,7 @@ bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double
                Stats& st, std::string& err, uint64_t set_stride = 0) {
   const uint64_t dim = 1ULL << s.nbits;
   const uint64_t stride = set_stride ? set_stride : dim;
+  if (cfg.c64 && !s.tiled) { err = "complex64 gradients need tile passes (at least 7 qubits)"; return false; }
   int gap = 0;
   if (s.tiled && stride != dim) {
     if (stride != 2 * dim) { err = "internal: tile passes over arrays spaced other than 2^(n+1) apart"; return false; }
@@ -467,6 +481,25 @@ bool run_shape(Workspace& w, const Cfg& cfg, const Shape& s, bool cached, double
           return false;
     st.launches += s.sops.size() * nsets;
     st.bytes += (uint64_t)s.sops.size() * nsets * (32ULL << s.nbits);
+    return true;
+  }
+  if (cfg.c64) {   // complex64: direct loads and stores, no tensor maps
+    for (size_t i = 0; i < s.plans.size(); ++i) {
+      PassDesc d = s.plans[i].desc;
+      d.gap = (uint8_t)gap;
+      d.set_shift = (uint32_t)log2_u64(d.ntiles);
+      d.ntiles *= nsets;
+      d.nsets = nsets;
+      d.set_mat_stride = mat_stride;
+      d.grad_stride = grad_stride;
+      if (grid) *grid = tile_pass_grid(d, cfg.tl, w.num_sms);
+      if (!cuda_ok(jit_launch_narrow(s.jit[i], d, mats, state, cfg.tl, w.num_sms, w.stream, gpart),
+                   "complex64 pass kernel", err))
+        return false;
+      ++st.jit_passes;
+    }
+    st.launches += s.plans.size();
+    st.bytes += (uint64_t)s.plans.size() * nsets * (16ULL << s.nbits);
     return true;
   }
   std::vector<CUtensorMap> scratch;
@@ -566,7 +599,9 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
       (!want_grad && !w.psi.ensure(dim * S, err, "the states", w.stream)))
     return false;
   const unsigned max_grid = (unsigned)w.num_sms * (unsigned)std::max(1, cfg.tl.ctas_per_sm);
-  if (want_grad && (!w.joint.ensure(jdim * S, err, "the joint arrays", w.stream) ||
+  // complex64 joint arrays take half the bytes (the buffer counts complex128 units)
+  const uint64_t joint_units = cfg.c64 ? (jdim * S + 1) / 2 : jdim * S;
+  if (want_grad && (!w.joint.ensure(joint_units, err, "the joint arrays", w.stream) ||
                     !w.gpart.ensure((size_t)std::max(ngrads, 1) * S * max_grid, err, "gradient partials", w.stream) ||
                     !w.gsum.ensure((size_t)std::max(ngrads, 1) * S, err, "gradient sums", w.stream)))
     return false;
@@ -611,13 +646,19 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
     // zero-padded to 2^7): the forward runs on the psi half in place, lambda =
     // H psi is written to the other half, and the backward sweep runs on the
     // whole array -- two state-sized buffers per set, no copy of psi.
-    if (!cuda_ok(launch_init_joint(w.joint.p, c.n, jdim, (int)S, w.stream), "reset", err)) return false;
+    float2* J64 = reinterpret_cast<float2*>(w.joint.p);   // the complex64 view (cfg.c64)
+    if (cfg.c64 ? !cuda_ok(launch_init_joint_c64(J64, c.n, jdim, (int)S, w.stream), "reset", err)
+                : !cuda_ok(launch_init_joint(w.joint.p, c.n, jdim, (int)S, w.stream), "reset", err))
+      return false;
     if (!run_shape(w, cfg, *fw, fw_cached, w.joint.p, S, dm, (uint32_t)nf, nullptr, 0, nullptr, st, err, jdim))
       return false;
     st.fw_passes += (fw->tiled ? fw->plans.size() : fw->sops.size()) * S;
-    if (!cuda_ok(launch_hamiltonian_joint(w.joint.p, jdim, c.n, (int)S, c.ham.groups, w.zmask.p, w.coef.p,
-                                          w.joint.p + dim, jdim, partials, energy_dev, w.stream),
-                 "Hamiltonian kernel", err))
+    if (cfg.c64 ? !cuda_ok(launch_hamiltonian_c64(J64, jdim, c.n, (int)S, c.ham.groups, w.zmask.p, w.coef.p, J64 + dim,
+                                                  jdim, partials, energy_dev, w.stream),
+                           "Hamiltonian kernel", err)
+                : !cuda_ok(launch_hamiltonian_joint(w.joint.p, jdim, c.n, (int)S, c.ham.groups, w.zmask.p, w.coef.p,
+                                                    w.joint.p + dim, jdim, partials, energy_dev, w.stream),
+                           "Hamiltonian kernel", err))
       return false;
     unsigned grid = 0;
     // partials of the sets a CTA never reaches stay zero
@@ -632,7 +673,7 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
     if (!cuda_ok(launch_row_sums(w.gpart.p, ngrads * (int)S, (int)grid, w.gsum.p, w.stream), "gradient sums", err))
       return false;
     st.launches += 6;
-    st.bytes += S * 32ULL * dim;   // read psi, write lambda
+    st.bytes += S * (cfg.c64 ? 16ULL : 32ULL) * dim;   // read psi, write lambda
   }
   double* ho = w.hout[k].p;
   if (!cuda_ok(cudaMemcpyAsync(ho, energy_dev, S * sizeof(double), cudaMemcpyDeviceToHost, w.stream), "D2H", err) ||
@@ -727,7 +768,7 @@ int current_device(std::string& err) {
   return dev;
 }
 
-thread_local double t_stats[9] = {0};
+thread_local double t_stats[10] = {0};
 
 // Workspaces kept between calls (streams, events and buffers are costly to
 // create and allocation synchronises the device).  A workspace holding more
@@ -760,14 +801,15 @@ void pool_give(Workspace* w, bool ok) {
 }
 
 // Run all jobs of `circs` (every parameter set of every circuit) on `nstreams` workers.
-int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool want_grad) {
+int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool want_grad, bool c64 = false) {
   const auto t0 = std::chrono::steady_clock::now();
   std::string err;
   const int dev = current_device(err);
   if (dev < 0) { record_error(E_DEVICE, err.c_str()); return -1; }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const Cfg cfg = Cfg::from_env();
+  Cfg cfg = Cfg::from_env();
+  cfg.c64 = c64;
   // jobs: a circuit's parameter sets in groups whose joint arrays ([psi |
   // lambda], 32 B x 2^n per set) fit the per-job budget; the energy-only path
   // (the plain baseline) runs one set per job on a state buffer (16 B x 2^n)
@@ -775,8 +817,31 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   std::vector<Job> jobs;
   const double job_bytes = env_double("IQ_ADJOINT_JOB_BYTES", 4.0 * (1ull << 30));
   Workspace::Bounds bd;
+  // circuits whose psi and lambda fit one CTA's shared memory go to the
+  // persistent executor (iq_resident.cu), all their sets in one launch
+  const int res_max = (want_grad && !c64)
+                          ? std::min(env_int("IQ_RESIDENT_MAX_QUBITS", kResidentMaxQubits), kResidentMaxQubits)
+                          : 0;
+  std::vector<ResidentJob> rjobs;
+  size_t resident_sets = 0;
   for (auto& c : circs) {
-    const double per_set = 16.0 * std::ldexp(1.0, joint_bits(c->n));
+    if (c->n <= res_max && c->nparams <= kResidentMaxParams && c->nsets > 0) {
+      ResidentJob r;
+      r.n = c->n;
+      r.ops = &c->ops;
+      r.nparams = c->nparams;
+      r.nsets = c->nsets;
+      r.params = c->params;
+      r.groups = &c->ham.groups;
+      r.zmask = &c->ham.zmask;
+      r.coef = &c->ham.coef;
+      r.energy_out = c->energy_out;
+      r.grad_out = c->grad_out;
+      rjobs.push_back(r);
+      resident_sets += c->nsets;
+      continue;
+    }
+    const double per_set = (c64 ? 8.0 : 16.0) * std::ldexp(1.0, joint_bits(c->n));
     const size_t group = want_grad ? (size_t)std::max(1.0, std::floor(job_bytes / per_set)) : 1;
     // per set: at most 3 rotations per gate, each at most a dense 4x4 (16
     // elements) forward and one backward; at most 3 gradient terms per gate
@@ -785,13 +850,25 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
       const size_t ns = std::min(group, c->nsets - s0);
       jobs.push_back({c.get(), s0, ns, (double)ns * std::ldexp((double)nops, c->n)});
       if (!want_grad) bd.psi_amps = std::max<uint64_t>(bd.psi_amps, (uint64_t)ns << c->n);
-      if (want_grad) bd.joint_amps = std::max<uint64_t>(bd.joint_amps, (uint64_t)ns << joint_bits(c->n));
+      if (want_grad)
+        bd.joint_amps = std::max<uint64_t>(bd.joint_amps, ((uint64_t)ns << joint_bits(c->n)) >> (c64 ? 1 : 0));
       bd.mats = std::max(bd.mats, ns * 96 * nops);
       bd.sets = std::max(bd.sets, ns);
       if (want_grad) bd.grads = std::max(bd.grads, ns * 3 * nops);
     }
   }
-  if (jobs.empty()) return 0;
+  std::string res_err;
+  bool res_ok = true;
+  // the persistent launch runs beside the workers' tile passes
+  std::thread res_thread;
+  if (!rjobs.empty()) res_thread = std::thread([&] {
+    cudaSetDevice(dev);
+    res_ok = resident_run(dev, rjobs, res_err);
+  });
+  struct JoinRes {
+    std::thread& t;
+    ~JoinRes() { if (t.joinable()) t.join(); }
+  } join_res{res_thread};
   // largest first
   std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) { return a.cost > b.cost; });
   // workers: as asked, no more than jobs, and as many workspaces as fit in 80% of free memory
@@ -830,13 +907,17 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
     }
     pool_give(wp, ok);
   };
-  if (nw == 1) {
+  if (jobs.empty()) {
+    nw = 0;
+  } else if (nw == 1) {
     worker(0);
   } else {
     std::vector<std::thread> th;
     for (int i = 0; i < nw; ++i) th.emplace_back(worker, i);
     for (auto& t : th) t.join();
   }
+  if (res_thread.joinable()) res_thread.join();
+  if (!res_ok && first_err.empty()) first_err = res_err;
   cudaSetDevice(dev);
   count_launches(st.launches.load());
   const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -849,6 +930,7 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   t_stats[6] = wall;
   t_stats[7] = (double)nw;
   t_stats[8] = (double)st.jit_passes.load();
+  t_stats[9] = (double)resident_sets;
   (void)st.replans;
   if (!first_err.empty()) {
     record_error(first_err.find("scheduler") == 0 ? E_STATE : E_CUDA, first_err.c_str());
@@ -880,7 +962,7 @@ bool load_circuit(const iq_adjoint_circuit& in, Circuit& c, bool want_grad, std:
   return true;
 }
 
-int run_circuits(const iq_adjoint_circuit* in, size_t count, int nstreams, bool want_grad) {
+int run_circuits(const iq_adjoint_circuit* in, size_t count, int nstreams, bool want_grad, bool c64 = false) {
   if (count && !in) { record_error(E_ARG, "null circuit array"); return -1; }
   std::vector<std::unique_ptr<Circuit>> circs;
   for (size_t i = 0; i < count; ++i) {
@@ -894,7 +976,7 @@ int run_circuits(const iq_adjoint_circuit* in, size_t count, int nstreams, bool 
     }
     circs.push_back(std::move(c));
   }
-  return run_batch(circs, nstreams, want_grad);
+  return run_batch(circs, nstreams, want_grad, c64);
 }
 
 // ------------------------------------------------------------ complex64 variant
@@ -1153,6 +1235,9 @@ int iq_adjoint_gradient_c64(size_t num_qubits, size_t num_ops, const int* kinds,
   c.paulis = paulis;
   c.energy_out = energy_out;
   c.grad_out = grad_out;
+  // from 7 qubits: the tile-pass executor with complex64 arrays (specialised
+  // kernels); below, or with IQ_C64_TILE=0, one pass per gate run (adjoint_c64)
+  if (num_qubits >= 7 && env_int("IQ_C64_TILE", 1) != 0) return run_circuits(&c, 1, 1, true, true);
   return adjoint_c64(c);
 }
 
@@ -1163,6 +1248,7 @@ int iq_adjoint_gradient_batch(const iq_adjoint_circuit* circuits, size_t num_cir
 int iq_ansatz_energy(const iq_adjoint_circuit* circuit) { return run_circuits(circuit, 1, 1, false); }
 
 int iq_adjoint_release(void) {
+  resident_release();
   std::vector<Workspace*> ws;
   {
     std::lock_guard<std::mutex> g(g_pool_mu);
@@ -1178,8 +1264,8 @@ int iq_adjoint_release(void) {
 
 int iq_adjoint_stats(double* out, size_t n) {
   if (!out) return -1;
-  for (size_t i = 0; i < n && i < 9; ++i) out[i] = t_stats[i];
-  return 9;
+  for (size_t i = 0; i < n && i < 10; ++i) out[i] = t_stats[i];
+  return 10;
 }
 
 }  // extern "C"

@@ -195,6 +195,7 @@ struct JitKernel {
   CUfunction fn = nullptr;
   int nt = 128;
   bool sets = false;     // shared-memory matrices per parameter set (interpreting kernel's arguments)
+  bool narrow = false;   // complex64 array, direct global loads and stores (jit_launch_narrow)
   std::atomic<int> smem_limit_set{0};
 };
 
@@ -277,6 +278,7 @@ bool install(int dev, const std::string& key, const std::string& src, const std:
   if (dr.getfn(&k->fn, k->mod, "iq_jit_pass") != CUDA_SUCCESS) { err = "cuModuleGetFunction failed"; return false; }
   k->nt = source_NT(src);
   k->sets = src.find(" sets=1 ") != std::string::npos;
+  k->narrow = src.find(" narrow=1 ") != std::string::npos;
   JitState& S = state();
   std::lock_guard<std::mutex> lk(S.mu);
   S.cache.emplace(std::make_pair(dev, key), std::move(k));   // keeps the first if two raced
@@ -330,7 +332,7 @@ bool jit_ready(std::string& err, int& dev) {
 }  // namespace
 
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks, int threads, bool set_mode) {
+                 int min_blocks, int threads, bool set_mode, bool narrow) {
   out.assign(passes.size(), nullptr);
   int dev = 0;
   if (!jit_ready(err, dev)) return false;
@@ -341,13 +343,13 @@ bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const J
     std::set<std::string> seen;
     std::lock_guard<std::mutex> lk(S.mu);
     for (size_t i = 0; i < passes.size(); ++i) {
-      keys[i] = jit_pass_key(*passes[i], min_blocks, threads, set_mode);
+      keys[i] = jit_pass_key(*passes[i], min_blocks, threads, set_mode, narrow);
       auto it = S.cache.find({dev, keys[i]});
       if (it != S.cache.end()) { out[i] = it->second.get(); continue; }
       if (S.cache.size() + todo.size() >= kMaxKernels) continue;
       if (!seen.insert(keys[i]).second) continue;
       std::string e;
-      srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode);
+      srcs[i] = jit_pass_source(*passes[i], e, min_blocks, threads, set_mode, narrow);
       if (!srcs[i].empty()) todo.push_back((int)i);
     }
   }
@@ -468,6 +470,27 @@ cudaError_t jit_launch_sets(const JitKernel* kc, const CUtensorMap& tm, const Pa
   }
   void* args[] = {const_cast<CUtensorMap*>(&tm), const_cast<PassDesc*>(&d), &dev_mats, &dev_status, &nbuf,
                   &grad_partials};
+  const unsigned grid = tile_pass_grid(d, tl, num_sms);
+  const CUresult r = dr.launch(k->fn, grid, 1, 1, (unsigned)k->nt, 1, 1, (unsigned)smem, (CUstream)st, args, nullptr);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;
+}
+
+cudaError_t jit_launch_narrow(const JitKernel* kc, const PassDesc& d, const double2* dev_mats, void* state,
+                              const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials) {
+  JitKernel* k = const_cast<JitKernel*>(kc);
+  if (!k->narrow) return cudaErrorInvalidValue;
+  if (d.ngrad && !grad_partials) return cudaErrorInvalidValue;
+  const Driver& dr = driver();
+  const size_t smem = 1024 + ((size_t)16 << d.M) + (size_t)d.mat_elems * 16 + (size_t)d.ngrad * (k->nt / 8) * 8;
+  if (!k->smem_limit_set.load(std::memory_order_acquire)) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (dr.setattr(k->fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, optin - 1024) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+    k->smem_limit_set.store(1, std::memory_order_release);
+  }
+  void* args[] = {const_cast<PassDesc*>(&d), &dev_mats, &state, &grad_partials};
   const unsigned grid = tile_pass_grid(d, tl, num_sms);
   const CUresult r = dr.launch(k->fn, grid, 1, 1, (unsigned)k->nt, 1, 1, (unsigned)smem, (CUstream)st, args, nullptr);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorLaunchFailure;

@@ -36,8 +36,9 @@ struct JitKernel;
 // threads: CTA size of the kernels (128, 256; 0 = by register slots).
 // set_mode: the shared-memory form (passes over parameter sets, adjoint steps;
 // launched with jit_launch_sets).
+// narrow (with set_mode): kernels for complex64 arrays (jit_launch_narrow).
 bool jit_prepare(const std::vector<const PassDesc*>& passes, std::vector<const JitKernel*>& out, std::string& err,
-                 int min_blocks, int threads, bool set_mode = false);
+                 int min_blocks, int threads, bool set_mode = false, bool narrow = false);
 
 // Kernels already compiled for these passes (null where none); with
 // queue_missing, the missing ones are queued for compilation on background
@@ -58,6 +59,12 @@ cudaError_t jit_launch(const JitKernel* k, const CUtensorMap& tm, const PassDesc
 cudaError_t jit_launch_sets(const JitKernel* k, const CUtensorMap& tm, const PassDesc& d, const double2* dev_mats,
                             int* dev_status, const TileLaunch& tl, int num_sms, cudaStream_t st,
                             double* grad_partials);
+
+// Launch a complex64 pass (jit_prepare with narrow): `state` is the float2
+// array (set s at state + s * 2^nbits, or the gap layout of PassDesc::gap),
+// dev_mats the device matrix pool, grad_partials as for jit_launch_sets.
+cudaError_t jit_launch_narrow(const JitKernel* k, const PassDesc& d, const double2* dev_mats, void* state,
+                              const TileLaunch& tl, int num_sms, cudaStream_t st, double* grad_partials);
 
 // Kernels compiled and cubins loaded from the cache directory so far.
 void jit_counters(uint64_t* compiled, uint64_t* loaded_from_disk);

@@ -26,9 +26,13 @@ std::string mat(uint32_t i) { return (g_set_mode ? "smat[" : "Mt.m[") + std::to_
 // thread holds (v's bit i = register slot i).  Every operation is written with
 // the interpreting kernel's expression for it (iq_tile.cuh), so the results
 // agree bit for bit.
-bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
+// gmode bit 0: the stage loads its registers from the complex64 array in
+// global memory (gst + tile base tb + physical offsets) instead of the tile;
+// bit 1: it stores them there.
+bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int gmode = 0) {
   const StageDesc& sd = d.st[s];
   const int R = d.R, NV = 1 << R;
+  const bool gload = gmode & 1, gstore = gmode & 2, use_smem = !(gload && gstore);
   std::ostringstream& o = g.o;
   uint32_t sb[kMaxK];
   for (int i = 0; i < R; ++i) sb[i] = swz(1u << sd.S[i]);
@@ -41,16 +45,27 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
   o << "    {  // stage " << s << "\n";
   o << "      const unsigned lo = ((unsigned)(lane8 & 1) << " << (int)sd.lane[0] << ") | ((unsigned)((lane8 >> 1) & 1) << "
     << (int)sd.lane[1] << ") | ((unsigned)((lane8 >> 2) & 1) << " << (int)sd.lane[2] << ");\n";
+  if (gload || gstore)   // physical offsets of the register slots' tile-local bits
+    for (int i = 0; i < R; ++i)
+      o << "      const unsigned long long q" << i << " = local_to_phys(" << (1u << sd.S[i]) << "u, P);\n";
+  auto goff = [&](int v) {
+    std::string x = "gb";
+    for (int i = 0; i < R; ++i)
+      if ((v >> i) & 1) x += " | q" + std::to_string(i);
+    return "gst + (" + x + ")";
+  };
   o << "      for (int u = octet; u < " << (1 << sd.nt) << "; u += " << NT / 8 << ") {\n";
   o << "        unsigned base = lo";
   for (int i = 0; i < sd.nt; ++i) o << " | ((((unsigned)u >> " << i << ") & 1u) << " << (int)sd.tb[i] << ")";
-  o << ";\n        base = swz(base);\n";
+  o << ";\n";
+  if (gload || gstore) o << "        const unsigned long long gb = tb + local_to_phys(base, P);\n";
+  o << "        base = swz(base);\n";
   // The swizzle only mixes bits 0..2: swz(base) ^ off = (swz(base) ^ (off & 7))
   // + (off & ~7), because above bit 2 the thread's and the slots' bits are
   // disjoint.  One pointer per distinct (off & 7) then reaches every register's
   // slot with a constant displacement.
   std::string ptr[8];
-  for (int v = 0; v < NV; ++v) {
+  for (int v = 0; v < NV && use_smem; ++v) {
     const uint32_t k = voffc(v) & 7u;
     if (!ptr[k].empty()) continue;
     ptr[k] = "p" + std::to_string(k);
@@ -60,7 +75,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
   std::vector<std::string> cur(NV);
   for (int v = 0; v < NV; ++v) {
     cur[v] = g.fresh();
-    o << "        const double2 " << cur[v] << " = " << at(v) << ";\n";
+    o << "        const double2 " << cur[v] << " = " << (gload ? "ldn(" + goff(v) + ")" : at(v)) << ";\n";
   }
   auto def = [&](const std::string& expr) {
     const std::string n = g.fresh();
@@ -234,7 +249,10 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
         return false;
     }
   }
-  for (int v = 0; v < NV; ++v) o << "        " << at(v) << " = " << cur[v] << ";\n";
+  for (int v = 0; v < NV; ++v) {
+    if (gstore) o << "        stn(" << goff(v) << ", " << cur[v] << ");\n";
+    else o << "        " << at(v) << " = " << cur[v] << ";\n";
+  }
   o << "      }\n    }\n    __syncthreads();\n";
   return true;
 }
@@ -243,14 +261,14 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err) {
 
 // Everything of `d` (and of the kernel form) that its generated source depends
 // on, as a compact byte string: equal keys give equal sources.
-std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode) {
+std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode, bool narrow) {
   std::string k;
   k.reserve(64 + d.nstages * 32 + d.nops * 16);
   auto put = [&](uint32_t v) { k.append(reinterpret_cast<const char*>(&v), sizeof(v)); };
   put(1);   // key format
   put((uint32_t)min_blocks);
   put((uint32_t)threads);
-  put(set_mode ? 1u : 0u);
+  put(set_mode ? (narrow ? 2u : 1u) : 0u);
   put(d.M);
   put(d.c);
   put(d.R);
@@ -277,7 +295,12 @@ std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool se
 }
 
 // Source of the kernel specialised to pass `d` (see iq_plan.h).
-std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads, bool set_mode) {
+std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks, int threads, bool set_mode,
+                            bool narrow) {
+  if (narrow && !set_mode) {
+    err = "complex64 passes use the shared-memory form";
+    return "";
+  }
   if (!set_mode && (d.ngrad || d.nsets > 1)) {
     err = "passes over several parameter sets need the shared-memory form";
     return "";
@@ -292,10 +315,31 @@ std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks,
   const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
   Gen g;
   std::ostringstream& o = g.o;
-  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " sets=" << (set_mode ? 1 : 0) << " M=" << (int)d.M
+  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " sets=" << (set_mode ? 1 : 0)
+    << " narrow=" << (narrow ? 1 : 0) << " M=" << (int)d.M
     << " c=" << (int)d.c << " R=" << (int)d.R
     << " stages=" << (int)d.nstages << " ops=" << d.nops << "\n";
   o << "#include \"iq_pipe.cuh\"\nusing namespace iqb;\n";
+  if (narrow) {
+    o << "struct JitStages {\n  const PassDesc& P;\n  float2* gst;\n  int lane8, octet;\n  unsigned omask;\n";
+    o << "  __device__ __forceinline__ void operator()(double2* tile, const double2* smat, double* gslots, "
+         "unsigned long long t) {\n";
+    o << "    const unsigned long long tb = tile_base(t, P);\n";
+    o << "    double* const gs = gslots + octet * " << d.ngrad << ";\n    (void)gs; (void)tile;\n";
+    for (int s = 0; s < d.nstages; ++s) {
+      const int gm = (s == 0 ? 1 : 0) | (s == d.nstages - 1 ? 2 : 0);
+      if (!gen_stage(g, d, s, NT, err, gm)) return "";
+    }
+    o << "  }\n};\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << MINB << ")\n"
+      << "iq_jit_pass(const __grid_constant__ PassDesc P, const double2* __restrict__ mats,\n"
+      << "            float2* __restrict__ state, double* __restrict__ grad_partials) {\n"
+      << "  extern __shared__ __align__(1024) unsigned char smem_raw[];\n"
+      << "  const int ctid = threadIdx.x;\n"
+      << "  JitStages st{P, state, ctid & 7, ctid >> 3, 0xFFu << (ctid & 24)};\n"
+      << "  direct_set_pass<" << NT << ">(P, mats, grad_partials, smem_raw, st);\n}\n";
+    return o.str();
+  }
   if (set_mode) {
     o << "struct JitStages {\n  int lane8, octet;\n  unsigned omask;\n";
     o << "  __device__ __forceinline__ void operator()(double2* tile, const double2* smat, double* gslots, bool work) {\n";

@@ -662,6 +662,62 @@ cudaError_t launch_init_joint(double2* s, int n, uint64_t jdim, int nsets, cudaS
   return cudaGetLastError();
 }
 
+// complex64 storage of the same: psi_s at psi + s * pstride (float2), lambda_s
+// written to lam + s * lstride (float2, rounded once), every product and sum in FP64
+__global__ void hamiltonian_c64_kernel(const float2* __restrict__ psi, uint64_t pstride, uint64_t dim, HamTerms h,
+                                       const uint64_t* __restrict__ zmask, const double2* __restrict__ coef,
+                                       float2* __restrict__ lam_out, uint64_t lstride, double* __restrict__ partials) {
+  psi += blockIdx.y * pstride;
+  if (lam_out) lam_out += blockIdx.y * lstride;
+  partials += (size_t)blockIdx.y * gridDim.x;
+  double e = 0.0;
+  for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < dim; x += (uint64_t)gridDim.x * blockDim.x) {
+    const float2 pf = psi[x];
+    const double2 px = make_double2(pf.x, pf.y);
+    double2 lam = make_double2(0.0, 0.0);
+    for (int g = 0; g < h.ngroups; ++g) {
+      const uint64_t src = x ^ h.xmask[g];
+      const float2 af = psi[src];
+      const double2 a = (h.xmask[g] == 0) ? px : make_double2(af.x, af.y);
+      double2 f = make_double2(0.0, 0.0);
+      for (int t = h.first[g]; t < h.first[g + 1]; ++t) {
+        const double2 c = coef[t];
+        if (__popcll(src & zmask[t]) & 1) { f.x -= c.x; f.y -= c.y; }
+        else { f.x += c.x; f.y += c.y; }
+      }
+      lam = cfma(lam, f, a);
+    }
+    if (lam_out) lam_out[x] = make_float2(__double2float_rn(lam.x), __double2float_rn(lam.y));
+    e += px.x * lam.x + px.y * lam.y;
+  }
+  e = block_sum(e);
+  if (threadIdx.x == 0) partials[blockIdx.x] = e;
+}
+
+cudaError_t launch_hamiltonian_c64(const float2* psi, uint64_t pstride, int n, int nsets, const HamTerms& h,
+                                   const uint64_t* zmask, const double2* coef, float2* lam, uint64_t lstride,
+                                   double* partials, double* energy, cudaStream_t st) {
+  if (nsets < 1) nsets = 1;
+  hamiltonian_c64_kernel<<<dim3(kRedBlocks, nsets), kRedThreads, 0, st>>>(psi, pstride, 1ULL << n, h, zmask, coef,
+                                                                          lam, lstride, partials);
+  row_sum_kernel<<<nsets, 256, 0, st>>>(partials, kRedBlocks, energy);
+  return cudaGetLastError();
+}
+
+__global__ void init_joint_c64_kernel(float2* __restrict__ s, uint64_t dim, uint64_t jdim, uint64_t total) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t l = i & (jdim - 1);
+    if (l < dim) s[i] = make_float2(l == 0 ? 1.0f : 0.0f, 0.0f);
+    else if (l >= 2 * dim) s[i] = make_float2(0.0f, 0.0f);
+  }
+}
+
+cudaError_t launch_init_joint_c64(float2* s, int n, uint64_t jdim, int nsets, cudaStream_t st) {
+  const uint64_t total = jdim * (uint64_t)(nsets < 1 ? 1 : nsets);
+  init_joint_c64_kernel<<<grid_for(total, 256), 256, 0, st>>>(s, 1ULL << n, jdim, total);
+  return cudaGetLastError();
+}
+
 // out[r] = sum_c in[r * cols + c], in order (one block per row)
 __global__ void row_sum_kernel(const double* __restrict__ in, int cols, double* __restrict__ out) {
   double v = 0.0;

@@ -105,6 +105,11 @@ cudaError_t launch_hamiltonian_joint(const double2* psi, uint64_t pstride, int n
 // nsets joint arrays [psi | lambda | zero padding] of jdim amplitudes end to
 // end: psi halves (2^n amplitudes) set to e_0, padding above 2^(n+1) zeroed.
 cudaError_t launch_init_joint(double2* s, int n, uint64_t jdim, int nsets, cudaStream_t st);
+// The same two with complex64 (float2) storage; products and sums in FP64.
+cudaError_t launch_hamiltonian_c64(const float2* psi, uint64_t pstride, int n, int nsets, const HamTerms& h,
+                                   const uint64_t* zmask, const double2* coef, float2* lam, uint64_t lstride,
+                                   double* partials, double* energy, cudaStream_t st);
+cudaError_t launch_init_joint_c64(float2* s, int n, uint64_t jdim, int nsets, cudaStream_t st);
 cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, cudaStream_t st);
 
 // Eigenvalues (ascending) of the reduced state on the kept qubits keep[0..k) of
@@ -113,6 +118,21 @@ cudaError_t launch_row_sums(const double* in, int rows, int cols, double* out, c
 int reduced_spectrum_max_bits();
 cudaError_t reduced_spectrum(const double2* psi, int nbits, const int* keep, int k, std::vector<double>& eig,
                              cudaStream_t st);
+
+// Measurement shots on the device (iq_sampling.cu): `shots` outcome indices
+// of the 2^nbits state into d_out, with the reference's random numbers
+// (mt19937_64 seeded with `seed`, uniform_real_distribution(0, 1)) and its
+// lower_bound rule.  work: sample_work_bytes(nbits, shots) bytes of device memory.
+size_t sample_work_bytes(int nbits, uint64_t shots);
+cudaError_t sample_on_device(const double2* s, int nbits, uint64_t shots, uint64_t seed, void* work, uint64_t* d_out,
+                             cudaStream_t st);
+// `count` uniform draws of the mt19937_64 stream seeded with `seed` (one CTA).
+cudaError_t launch_mt64_uniform(uint64_t seed, uint64_t count, double* out, cudaStream_t st);
+// Sorted distinct outcomes of d_shots and their counts (d_nuniq: how many).
+// work: count_work_bytes(shots) bytes.
+size_t count_work_bytes(uint64_t shots);
+cudaError_t count_outcomes(const uint64_t* d_shots, uint64_t shots, void* work, uint64_t* d_vals, uint64_t* d_cnts,
+                           uint64_t* d_nuniq, cudaStream_t st);
 
 // Record an error for iq_last_error (defined in iq_runtime.cu).
 void record_error(int code, const char* msg);

@@ -424,4 +424,70 @@ __device__ __forceinline__ void set_tile_pass(const CUtensorMap& tm, const PassD
   }
 }
 
+// ---- passes over complex64 (float2) arrays: the first stage loads its
+// registers straight from global memory (widened to FP64), the last stage
+// stores them there (rounded once to FP32), and the stages between exchange
+// through a shared-memory tile of double2 as in the TMA pipeline.  Every CTA
+// walks its tiles (blockIdx.x, + gridDim.x, ...); no asynchronous copies.
+
+// Physical index bits of tile-local index L: bits below c are themselves, bit
+// c + i is H[i].
+__device__ __forceinline__ unsigned long long local_to_phys(uint32_t L, const PassDesc& P) {
+  unsigned long long x = L & ((1u << P.c) - 1u);
+  for (int i = 0; i < P.nH; ++i)
+    if ((L >> (P.c + i)) & 1u) x |= 1ULL << P.H[i];
+  return x;
+}
+__device__ __forceinline__ double2 ldn(const float2* p) {
+  const float2 v = *p;
+  return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void stn(float2* p, double2 v) {
+  *p = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+}
+
+// Dynamic shared memory: [one double2 tile][the current set's matrix block]
+// [gradient accumulators: one row of ngrad per octet].  stages(tile, smat,
+// gslots, t) runs the pass's stages on tile t (each stage ends with a
+// __syncthreads()).  Set switches as in SetTileBody.
+template <int NT, class Stages>
+__device__ __forceinline__ void direct_set_pass(const PassDesc& P, const double2* mats, double* grad_partials,
+                                                unsigned char* smem_raw, Stages& stages) {
+  double2* tile = aligned_tiles(smem_raw);
+  double2* smat = tile + (1u << P.M);
+  double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
+  const int tid = threadIdx.x;
+  const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
+  uint32_t cur_set = (blockIdx.x < P.ntiles) ? (uint32_t)(blockIdx.x >> sshift) : 0u;
+  for (uint32_t i = tid; i < P.mat_elems; i += NT) smat[i] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + i];
+  for (uint32_t i = tid; i < P.ngrad * (NT / 8); i += NT) gslots[i] = 0.0;
+  __syncthreads();
+  auto flush = [&]() {
+    for (uint32_t i = tid; i < P.ngrad; i += NT) {
+      double v = 0.0;
+      for (int o = 0; o < NT / 8; ++o) v += gslots[o * P.ngrad + i];
+      grad_partials[((size_t)cur_set * P.grad_stride + P.grad_term[i]) * gridDim.x + blockIdx.x] = v;
+    }
+  };
+  for (unsigned long long t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+    const uint32_t tset = (uint32_t)(t >> sshift);
+    if (tset != cur_set) {
+      if (P.ngrad) {
+        flush();
+        __syncthreads();
+        for (uint32_t j = tid; j < P.ngrad * (NT / 8); j += NT) gslots[j] = 0.0;
+      }
+      cur_set = tset;
+      for (uint32_t j = tid; j < P.mat_elems; j += NT)
+        smat[j] = mats[P.mat_base + (size_t)cur_set * P.set_mat_stride + j];
+      __syncthreads();
+    }
+    stages(tile, smat, gslots, t);
+  }
+  if (P.ngrad) {
+    __syncthreads();
+    flush();
+  }
+}
+
 }  // namespace iqb

@@ -334,12 +334,15 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 // set_mode: the form for passes over several parameter sets and adjoint steps
 // (matrices staged per set in shared memory, gradient accumulators; the
 // interpreting kernel's launch arguments); otherwise matrices are a kernel
-// parameter block.
+// parameter block.  narrow (with set_mode): the array is complex64 (float2);
+// the first stage loads from and the last stores to global memory directly,
+// widening to FP64 and rounding once (arguments: pass, matrices, state,
+// gradient partials; launched with jit_launch_narrow).
 std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2, int threads = 0,
-                            bool set_mode = false);
+                            bool set_mode = false, bool narrow = false);
 // Compact byte string of everything jit_pass_source's output depends on
 // (equal keys give equal sources): the kernel cache's key.
-std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode);
+std::string jit_pass_key(const PassDesc& d, int min_blocks, int threads, bool set_mode, bool narrow = false);
 struct cplx64 { double re, im; };
 // Fuse runs of queued operations on at most two qubits into single 4x4 blocks
 // (a two-qubit operation absorbs the open one-qubit blocks of its qubits and

@@ -892,52 +892,75 @@ void iq_statevector_sample(void* sv, size_t num_shots, uint64_t seed, uint64_t* 
   if (!e || !results_out) return;
   if (!e->sync()) return;
   if (num_shots == 0) return;
-  const int bb = std::min(12, e->nbits);
-  const uint64_t nblk = e->dim >> bb;
-  // device: block sums -> host prefix -> per-shot block, base, target -> device search
-  const size_t need = nblk * 8 + num_shots * 24 + 64;
-  void* dbuf = nullptr;
-  if (!cuda_ok(cudaMallocAsync(&dbuf, need + num_shots * 8, e->stream), "cudaMallocAsync sampling")) return;
-  double* d_bs = reinterpret_cast<double*>(dbuf);
-  uint64_t* d_blk = reinterpret_cast<uint64_t*>(d_bs + nblk);
-  double* d_base = reinterpret_cast<double*>(d_blk + num_shots);
-  double* d_tgt = d_base + num_shots;
-  uint64_t* d_out = reinterpret_cast<uint64_t*>(d_tgt + num_shots);
-  g_launches += 2;
-  e->st_launches += 2;
-  std::vector<double> bs(nblk);
-  bool ok = cuda_ok(launch_block_sums(e->d_state, e->dim, bb, d_bs, e->stream), "block sums") &&
-            cuda_ok(cudaMemcpyAsync(bs.data(), d_bs, nblk * 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
-            cuda_ok(cudaStreamSynchronize(e->stream), "sync");
-  if (ok) {
-    std::vector<double> incl(nblk);
-    double cum = 0.0;
-    for (uint64_t b = 0; b < nblk; ++b) {
-      cum += bs[b];
-      incl[b] = cum;
-    }
-    std::vector<uint64_t> blk(num_shots);
-    std::vector<double> base(num_shots), tgt(num_shots);
-    std::mt19937_64 rng(seed);                       // statevector.cpp:244-245
-    std::uniform_real_distribution<double> dist(0.0, 1.0);
-    for (size_t s = 0; s < num_shots; ++s) {
-      const double r = dist(rng);
-      uint64_t b = (uint64_t)(std::lower_bound(incl.begin(), incl.end(), r) - incl.begin());
-      if (b >= nblk) b = nblk - 1;
-      blk[s] = b;
-      base[s] = b ? incl[b - 1] : 0.0;
-      tgt[s] = r;
-    }
-    ok = cuda_ok(cudaMemcpyAsync(d_blk, blk.data(), num_shots * 8, cudaMemcpyHostToDevice, e->stream), "H2D") &&
-         cuda_ok(cudaMemcpyAsync(d_base, base.data(), num_shots * 8, cudaMemcpyHostToDevice, e->stream), "H2D") &&
-         cuda_ok(cudaMemcpyAsync(d_tgt, tgt.data(), num_shots * 8, cudaMemcpyHostToDevice, e->stream), "H2D") &&
-         cuda_ok(launch_block_search(e->d_state, bb, d_blk, d_base, d_tgt, d_out, (int)num_shots, e->stream),
-                 "block search") &&
-         cuda_ok(cudaMemcpyAsync(results_out, d_out, num_shots * 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
-         cuda_ok(cudaStreamSynchronize(e->stream), "sync");
+  if (num_shots > (size_t)INT32_MAX) {
+    set_error(E_ARG, "sample: %zu shots exceed the supported count", num_shots);
+    return;
   }
+  // everything on the device (iq_sampling.cu): block sums, their prefix, the
+  // mt19937_64 stream (statevector.cpp:244-245), per-shot search
+  const size_t wbytes = sample_work_bytes(e->nbits, num_shots);
+  void* dbuf = nullptr;
+  if (!cuda_ok(cudaMallocAsync(&dbuf, wbytes + num_shots * 8 + 256, e->stream), "cudaMallocAsync sampling")) return;
+  uint64_t* d_out = reinterpret_cast<uint64_t*>(static_cast<char*>(dbuf) + ((wbytes + 255) & ~(size_t)255));
+  ++e->st_launches;
+  cuda_ok(sample_on_device(e->d_state, e->nbits, num_shots, seed, dbuf, d_out, e->stream), "sampling") &&
+      cuda_ok(cudaMemcpyAsync(results_out, d_out, num_shots * 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
+      cuda_ok(cudaStreamSynchronize(e->stream), "sync");
   cudaFreeAsync(dbuf, e->stream);
   cudaStreamSynchronize(e->stream);
+}
+
+int iq_statevector_sample_counts(void* sv, size_t num_shots, uint64_t seed, uint64_t* values_out,
+                                 uint64_t* counts_out, size_t* num_unique) {
+  Engine* e = as_engine(sv, 0);
+  if (!e || !values_out || !counts_out || !num_unique) return -1;
+  *num_unique = 0;
+  if (!e->sync()) return -1;
+  if (num_shots == 0) return 0;
+  if (num_shots > ((size_t)1 << 30)) {
+    set_error(E_ARG, "sample_counts: %zu shots exceed the supported count (2^30)", num_shots);
+    return -1;
+  }
+  const size_t wbytes = (std::max(sample_work_bytes(e->nbits, num_shots), count_work_bytes(num_shots)) + 255) & ~(size_t)255;
+  const size_t obytes = (num_shots * 8 + 255) & ~(size_t)255;
+  char* dbuf = nullptr;
+  if (!cuda_ok(cudaMallocAsync(reinterpret_cast<void**>(&dbuf), wbytes + 3 * obytes + 256, e->stream),
+               "cudaMallocAsync sampling"))
+    return -1;
+  uint64_t* d_shots = reinterpret_cast<uint64_t*>(dbuf + wbytes);
+  uint64_t* d_vals = reinterpret_cast<uint64_t*>(dbuf + wbytes + obytes);
+  uint64_t* d_cnts = reinterpret_cast<uint64_t*>(dbuf + wbytes + 2 * obytes);
+  uint64_t* d_n = reinterpret_cast<uint64_t*>(dbuf + wbytes + 3 * obytes);
+  uint64_t nu = 0;
+  bool ok = cuda_ok(sample_on_device(e->d_state, e->nbits, num_shots, seed, dbuf, d_shots, e->stream), "sampling") &&
+            cuda_ok(count_outcomes(d_shots, num_shots, dbuf, d_vals, d_cnts, d_n, e->stream), "counts") &&
+            cuda_ok(cudaMemcpyAsync(&nu, d_n, 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
+            cuda_ok(cudaStreamSynchronize(e->stream), "sync");
+  if (ok)
+    ok = cuda_ok(cudaMemcpyAsync(values_out, d_vals, nu * 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
+         cuda_ok(cudaMemcpyAsync(counts_out, d_cnts, nu * 8, cudaMemcpyDeviceToHost, e->stream), "D2H") &&
+         cuda_ok(cudaStreamSynchronize(e->stream), "sync");
+  cudaFreeAsync(dbuf, e->stream);
+  cudaStreamSynchronize(e->stream);
+  if (!ok) return -1;
+  *num_unique = (size_t)nu;
+  return 0;
+}
+
+int iq_mt64_uniform(uint64_t seed, size_t count, double* out) {
+  if (!out) return -1;
+  if (count == 0) return 0;
+  double* d = nullptr;
+  cudaStream_t st = nullptr;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream")) return -1;
+  bool ok = cuda_ok(cudaMallocAsync(reinterpret_cast<void**>(&d), count * 8, st), "cudaMallocAsync") &&
+            cuda_ok(launch_mt64_uniform(seed, count, d, st), "mt19937_64") &&
+            cuda_ok(cudaMemcpyAsync(out, d, count * 8, cudaMemcpyDeviceToHost, st), "D2H") &&
+            cuda_ok(cudaStreamSynchronize(st), "sync");
+  if (d) cudaFreeAsync(d, st);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return ok ? 0 : -1;
 }
 
 double iq_statevector_entropy(void* sv, const size_t* qubits, size_t num_subsys_qubits) {

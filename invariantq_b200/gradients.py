@@ -209,10 +209,10 @@ def adjoint_release() -> int:
 def adjoint_stats() -> dict:
     """Counters of this thread's last adjoint / energy call."""
     lib = _lib.load()
-    out = (ctypes.c_double * 9)()
-    lib.iq_adjoint_stats(out, 9)
+    out = (ctypes.c_double * 10)()
+    lib.iq_adjoint_stats(out, 10)
     keys = ["jobs", "forward_passes", "backward_passes", "launches", "bytes", "host_ms", "wall_ms", "streams",
-            "specialised_passes"]
+            "specialised_passes", "resident_sets"]
     return dict(zip(keys, list(out)))
 
 

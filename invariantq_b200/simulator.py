@@ -213,9 +213,10 @@ class StateVectorSimulator:
                 total = float(np.sum(probs_vec))
                 if not np.isfinite(total) or total <= 0.0:
                     raise ValueError("non-unitary trajectory produced an invalid state norm")
-                samples = np.random.default_rng(seed).choice(1 << n, size=shots, p=probs_vec / total)
-            else:
-                samples = sv.sample(shots, seed)
+                counts = _counts(np.random.default_rng(seed).choice(1 << n, size=shots, p=probs_vec / total), n)
+            else:   # shots sampled and counted on the device
+                vals, cnts = sv.sample_counts(shots, seed)
+                counts = {format(int(v), f"0{n}b"): int(c) for v, c in zip(vals, cnts)}
             if ctx is not None:
                 ctx.check()
             stats = sv.stats()
@@ -225,7 +226,7 @@ class StateVectorSimulator:
                 ctx.__exit__(None, None, None)
         exec_ms = (time.perf_counter() - t0) * 1000.0
         return ExecutionResult(
-            counts=_counts(samples, n), probabilities=_prob_dict(probs_vec, n), statevector=amps,
+            counts=counts, probabilities=_prob_dict(probs_vec, n), statevector=amps,
             entanglement_entropy=entropy, execution_time_ms=exec_ms, backend_used="statevector",
             memory_used_bytes=mem_bytes, shots=shots,
             metadata={"num_qubits": n, "dimension": 1 << n, "allow_non_unitary": allow_non_unitary,

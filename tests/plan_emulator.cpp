@@ -533,7 +533,7 @@ extern "C" int emu_jit_sources(int nbits, int M, int c, int R, int max_stages, d
 // "//@@PASS@@".  Returns the number of passes, or -1 (message in `out`).
 extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
                                    const double* params, int M, int c, int R, int max_stages, double budget,
-                                   char* out, long long outlen) {
+                                   int narrow, char* out, long long outlen) {
   std::vector<AnsatzOp> ops(nops);
   for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
   std::string err, all;
@@ -565,7 +565,7 @@ extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int*
     std::vector<cplx64> packed;
     pack_pass_matrices(plans, pool.data(), packed);
     for (const PassPlan& pl : plans) {
-      const std::string s = jit_pass_source(pl.desc, err, 2, 0, true);
+      const std::string s = jit_pass_source(pl.desc, err, 2, 0, true, narrow != 0);
       if (s.empty()) {
         snprintf(out, (size_t)outlen, "%s", err.c_str());
         return -1;

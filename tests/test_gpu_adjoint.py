@@ -27,12 +27,21 @@ def G():
     return gradients
 
 
+@pytest.fixture(params=["resident", "tile"])
+def path(request, monkeypatch):
+    """Circuits of <= 12 qubits run on the persistent shared-memory executor by
+    default; 'tile' sends them through the tile-pass executor instead."""
+    if request.param == "tile":
+        monkeypatch.setenv("IQ_RESIDENT_MAX_QUBITS", "0")
+    return request.param
+
+
 def ansatz_of(G, n, ops):
     return G.Ansatz(n, [(k, (a,) if b < 0 else (a, b), p) for k, a, b, p in ops])
 
 
 @pytest.mark.parametrize("n,layers,seed", [(3, 2, 0), (6, 2, 1), (8, 3, 2), (11, 2, 3)])
-def test_tfim_gradient_vs_oracle(G, port, n, layers, seed):
+def test_tfim_gradient_vs_oracle(G, port, path, n, layers, seed):
     rng = np.random.default_rng(seed)
     ops = ar.tfim_ops(n, layers)
     th = rng.uniform(0, 2 * np.pi, ar.n_params(ops))
@@ -44,7 +53,7 @@ def test_tfim_gradient_vs_oracle(G, port, n, layers, seed):
 
 
 @pytest.mark.parametrize("n,ngates,seed", [(2, 20, 4), (5, 50, 5), (7, 80, 6), (9, 120, 7)])
-def test_mixed_gates_gradient_vs_oracle(G, port, n, ngates, seed):
+def test_mixed_gates_gradient_vs_oracle(G, port, path, n, ngates, seed):
     """RX/RY/RZ/U3/P rotations among H/SX/CZ/CX, and Y terms in H."""
     rng = np.random.default_rng(seed)
     ops = ar.random_ansatz(rng, n, ngates)
@@ -87,7 +96,7 @@ def test_batch_matches_single_jobs(G):
         jobs.append((a, h, rng.uniform(0, 2 * np.pi, (3, a.num_params))))
     out = G.adjoint_gradient_batch(jobs, num_streams=4)
     st = G.adjoint_stats()
-    assert st["jobs"] == 15 and st["streams"] == 4
+    assert st["resident_sets"] == 12 and st["jobs"] == 3   # the 13-qubit circuit's sets on the tile path
     out1 = G.adjoint_gradient_batch(jobs, num_streams=1)
     for (e, g), (e1, g1) in zip(out, out1):
         assert np.array_equal(e, e1) and np.array_equal(g, g1)
@@ -115,8 +124,10 @@ def test_batched_sets_at_scale(G):
     assert abs(e2 - e[7]) < 1e-13 and np.max(np.abs(g2 - g[7])) < 1e-12
 
 
-def test_structure_change_across_sets_is_replanned(G, port):
-    """An angle of 0 turns a fused block monomial: that set gets its own plan."""
+def test_structure_change_across_sets_is_replanned(G, port, monkeypatch):
+    """An angle of 0 turns a fused block monomial: that set gets its own plan
+    (tile-pass executor)."""
+    monkeypatch.setenv("IQ_RESIDENT_MAX_QUBITS", "0")
     n, ops = 8, ar.tfim_ops(8, 2)
     coeffs, paulis = tfim_terms(n, 1.0)
     a, h = ansatz_of(G, n, ops), G.PauliHamiltonian(n, coeffs, paulis)
@@ -165,6 +176,7 @@ def test_specialised_kernels_equal_interpreting(G, monkeypatch):
     (interpreting kernel) run the same plans with the same arithmetic:
     energies and gradients are identical, for one set and for sets batched
     in one launch (adjoint steps, set switches, gradient accumulators)."""
+    monkeypatch.setenv("IQ_RESIDENT_MAX_QUBITS", "0")
     rng = np.random.default_rng(31)
     jobs = []
     for n, L in [(12, 3), (9, 2)]:
@@ -180,3 +192,31 @@ def test_specialised_kernels_equal_interpreting(G, monkeypatch):
     for (e0, g0), (e1, g1) in zip(out["0"], out["1"]):
         assert np.array_equal(e0, e1) and np.array_equal(g0, g1)
     assert out["0s"][0] == out["1s"][0] and np.array_equal(out["0s"][1], out["1s"][1])
+
+
+def test_resident_executor_matches_tile_executor(G, monkeypatch):
+    """The persistent shared-memory executor (all sets of all circuits of <= 12
+    qubits in one launch from a device-side queue, replayed from a captured
+    graph) against the tile-pass executor on the same batch: 1e-12; the second
+    call of the same structure (graph replay, new parameters staged) equals a
+    fresh single-set run exactly, and the results do not depend on the batch."""
+    rng = np.random.default_rng(41)
+    jobs = []
+    for n, L in [(3, 2), (12, 2), (8, 3), (1, 2), (10, 1), (5, 4)]:
+        a = G.Ansatz.hardware_efficient(n, L) if n > 1 else G.Ansatz(1, [("ry", (0,), 0), ("rz", (0,), 1)])
+        jobs.append((a, G.PauliHamiltonian.tfim(n, 0.9), rng.uniform(0, 2 * np.pi, (5, a.num_params))))
+    res = G.adjoint_gradient_batch(jobs)
+    assert G.adjoint_stats()["resident_sets"] == 30
+    monkeypatch.setenv("IQ_RESIDENT_MAX_QUBITS", "0")
+    tile = G.adjoint_gradient_batch(jobs)
+    assert G.adjoint_stats()["resident_sets"] == 0
+    monkeypatch.delenv("IQ_RESIDENT_MAX_QUBITS")
+    for (e0, g0), (e1, g1) in zip(res, tile):
+        assert np.max(np.abs(e0 - e1)) < 1e-12 and np.max(np.abs(g0 - g1)) < 1e-12
+    jobs2 = [(a, h, P[::-1].copy()) for a, h, P in jobs]        # same structure, other parameters
+    res2 = G.adjoint_gradient_batch(jobs2)
+    for (e0, g0), (e2, g2) in zip(res, res2):
+        assert np.array_equal(e0[::-1], e2) and np.array_equal(g0[::-1], g2)
+    a, h, P = jobs[1]
+    e1, g1 = G.adjoint_gradient(a, h, P[3])
+    assert e1 == res[1][0][3] and np.array_equal(g1, res[1][1][3])

@@ -46,3 +46,23 @@ def test_mixed_gates_c64_vs_c128(G, n, ngates, seed):
     print(f"mixed n={n}: energy {abs(e - e32):.2e} gradient {np.max(np.abs(g - g32)):.2e}")
     assert abs(e - e32) < TOL
     assert np.max(np.abs(g - g32)) < TOL
+
+
+def test_tile_path_vs_per_run_passes(G, monkeypatch):
+    """From 7 qubits the complex64 gradient runs on the tile-pass executor
+    (specialised kernels loading float2 amplitudes, FP64 through the stages,
+    one rounding per pass); the per-run path (IQ_C64_TILE=0) rounds after every
+    run of gates.  Both against complex128: the tile path is the closer one."""
+    n = 16
+    a, h = G.Ansatz.hardware_efficient(n, 4), G.PauliHamiltonian.tfim(n, 0.9)
+    th = np.random.default_rng(16).uniform(0, 2 * np.pi, a.num_params)
+    e, g = G.adjoint_gradient(a, h, th)
+    et, gt = G.adjoint_gradient_c64(a, h, th)
+    st = G.adjoint_stats()
+    assert st["specialised_passes"] > 0 and st["forward_passes"] > 0
+    monkeypatch.setenv("IQ_C64_TILE", "0")
+    er, gr = G.adjoint_gradient_c64(a, h, th)
+    err_tile, err_run = np.max(np.abs(gt - g)), np.max(np.abs(gr - g))
+    print(f"c64 tile path {err_tile:.2e}, per-run path {err_run:.2e}")
+    assert abs(et - e) < TOL and err_tile < TOL and err_run < TOL
+    assert err_tile <= err_run

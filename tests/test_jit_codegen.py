@@ -109,3 +109,34 @@ def test_brickwall_kernel_compiles(emu):
     srcs = sources(emu, n, ops, M=11, budget=120.0)
     rc, log, size = compile_nvrtc(lib, max(srcs, key=len))
     assert rc == 0, log[:3000]
+
+
+@pytest.mark.parametrize("narrow", [0, 1])
+def test_adjoint_kernels_compile(emu, narrow):
+    """The shared-memory form the adjoint executor runs (parameter sets,
+    adjoint steps with gradient accumulators), for complex128 arrays through
+    the TMA pipeline and for complex64 arrays with direct loads and stores."""
+    from tests import adjoint_ref as ar
+    lib = nvrtc_lib()
+    if lib is None:
+        pytest.skip("libnvrtc not available")
+    n = 12
+    ops = ar.tfim_ops(n, 2)
+    th = np.random.default_rng(4).uniform(0, 2 * np.pi, ar.n_params(ops))
+    k = np.array([o[0] for o in ops], np.int32)
+    q0 = np.array([o[1] for o in ops], np.int32)
+    q1 = np.array([o[2] for o in ops], np.int32)
+    pi = np.array([o[3] for o in ops], np.int32)
+    buf = ctypes.create_string_buffer(64 << 20)
+    P = ctypes.c_void_p
+    rc = emu.emu_adjoint_sources(n, len(ops), P(k.ctypes.data), P(q0.ctypes.data), P(q1.ctypes.data),
+                                 P(pi.ctypes.data), P(th.ctypes.data), 12, 4, 4, 8, ctypes.c_double(160.0), narrow,
+                                 buf, ctypes.c_longlong(len(buf)))
+    text = buf.value.decode()
+    assert rc > 0, text
+    srcs = text.split("\n//@@PASS@@\n")
+    assert all(("narrow=1" in s) == bool(narrow) for s in srcs)
+    for s in (srcs[0], max(srcs, key=len)):
+        rc, log, size = compile_nvrtc(lib, s)
+        assert rc == 0, log[:3000]
+        assert size > 0
