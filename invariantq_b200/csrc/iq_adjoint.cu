@@ -70,6 +70,9 @@ struct Cfg {
   // complex64 states: every pass a specialised kernel that widens the loaded
   // amplitudes to FP64 and rounds once on store (jit_launch_narrow)
   bool c64 = false;
+  // a circuit with one parameter set: forward and backward in the forms that
+  // depend on its angles (fewer FP64 operations; adjoint_ops' single_set)
+  bool single_forms = true;
   static Cfg from_env() {
     Cfg c;
     c.jit = env_int("IQ_ADJOINT_JIT", 1);
@@ -87,6 +90,7 @@ struct Cfg {
     c.tl.ctas_per_sm = env_int("IQ_CTAS_PER_SM", 3);
     c.tl.consumers = 128;
     c.fuse = env_int("IQ_FUSE", 1);
+    c.single_forms = env_int("IQ_ADJOINT_SINGLE_FORMS", 1) != 0;
     return c;
   }
 };
@@ -165,7 +169,8 @@ struct Shape {
 
 bool same_op(const SchedOp& a, const SchedOp& b) {
   if (a.k != b.k || a.mono != b.mono || a.perm != b.perm || a.unit != b.unit || a.mat != b.mat ||
-      a.dense != b.dense || a.grad != b.grad || a.gen != b.gen || a.gidx != b.gidx)
+      a.dense != b.dense || a.grad != b.grad || a.gen != b.gen || a.gidx != b.gidx || a.rot != b.rot ||
+      a.norm != b.norm || a.urows != b.urows)
     return false;
   for (int i = 0; i < a.k; ++i)
     if (a.q[i] != b.q[i]) return false;
@@ -257,22 +262,14 @@ struct Circuit {
   std::unique_ptr<Shape> fw, bw;
 };
 
-// fused forward / backward operation lists and matrix pools of one parameter set
-struct JobOps {
-  std::vector<SchedOp> fw, bw;
-  std::vector<cplx64> fpool, bpool;
-  std::vector<int> grad_param;
-};
+// fused forward / backward operation lists and matrix pools of one parameter
+// set.  A circuit with a single parameter set takes the angle-dependent forms
+// (rotation + phase forward, scaled adjoint steps: adjoint_ops' single_set):
+// its plans serve no other set.
+using JobOps = AdjointOps;
 
 void job_ops(const Cfg& cfg, const Circuit& c, const double* theta, bool backward, JobOps& j) {
-  j.fw.clear(); j.bw.clear(); j.fpool.clear(); j.bpool.clear(); j.grad_param.clear();
-  std::vector<SchedOp> raw;
-  ansatz_forward(c.n, c.ops, theta, raw, j.fpool);
-  j.fw = cfg.fuse ? fuse_two_qubit_blocks(raw, j.fpool) : raw;
-  if (!backward) return;
-  raw.clear();
-  ansatz_backward(c.n, c.ops, theta, raw, j.bpool, j.grad_param, c.n);   // select bit n: [psi | lambda]
-  j.bw = cfg.fuse ? fuse_two_qubit_blocks(raw, j.bpool) : raw;
+  adjoint_ops(c.n, c.ops, theta, backward, cfg.fuse != 0, cfg.single_forms && c.nsets == 1, j);
 }
 
 int joint_bits(int n) { return std::max(n + 1, 7); }
@@ -336,6 +333,7 @@ struct Pending {
   Circuit* c = nullptr;
   std::vector<size_t> sets;   // parameter sets in launch order (device set k = sets[k])
   std::vector<int> grad_param;
+  std::vector<double> grad_scale;   // per set, ngrads factors of the scaled adjoint steps (empty: all 1)
   int ngrads = 0;
   bool grad = false;
 };
@@ -555,7 +553,12 @@ bool finish(Workspace& w, int k, std::string& err) {
       double* g = c.grad_out + set * (size_t)c.nparams;
       for (int i = 0; i < c.nparams; ++i) g[i] = 0.0;
       const double* row = out + S + j * (size_t)p.ngrads;
-      for (int t = 0; t < p.ngrads; ++t) g[p.grad_param[t]] += row[t];
+      if (p.grad_scale.empty()) {
+        for (int t = 0; t < p.ngrads; ++t) g[p.grad_param[t]] += row[t];
+      } else {
+        const double* sc = p.grad_scale.data() + j * (size_t)p.ngrads;
+        for (int t = 0; t < p.ngrads; ++t) g[p.grad_param[t]] += row[t] * sc[t];
+      }
     }
   }
   return true;
@@ -691,6 +694,17 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
   p.grad = want_grad;
   p.ngrads = ngrads;
   p.grad_param = want_grad ? jo[0].grad_param : std::vector<int>();
+  p.grad_scale.clear();
+  bool unit_scales = true;
+  for (uint32_t j = 0; j < S && want_grad; ++j)
+    for (double f : jo[j].grad_scale) unit_scales = unit_scales && f == 1.0;
+  if (!unit_scales)   // scaled adjoint steps: each term's scale in the order the backward passes run them
+    for (uint32_t j = 0; j < S; ++j) {
+      std::vector<double> sc;
+      exec_grad_scales(bw->tiled ? &bw->plans : nullptr, jo[j].bw, sc);
+      if ((int)sc.size() != ngrads) { err = "internal: gradient scales"; return false; }
+      p.grad_scale.insert(p.grad_scale.end(), sc.begin(), sc.end());
+    }
   st.jobs += S;
   return true;
 }

@@ -221,7 +221,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
       case OP_GRAD2: {   // adjoint step: select bit in slot 0, qubit in slot b (shared-memory matrices only)
         if (!g_set_mode) { err = "adjoint steps need the shared-memory form"; return false; }
         const int B = 1 << od.b;
-        const std::string G = std::to_string((int)od.perm);
+        const std::string G = std::to_string((int)od.perm) + ", " + std::to_string((int)od.flags);   // generator, form
         const std::string acc = g.fresh(), u0 = g.fresh(), u1 = g.fresh(), u3 = g.fresh();
         o << "        const double2 " << u0 << " = " << mat(m + 0) << ", " << u1 << " = " << mat(m + 1) << ", " << u3
           << " = " << mat(m + 3) << ";\n";
@@ -229,7 +229,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
         for (int v = 0; v < NV; ++v) {
           if (v & (1 | B)) continue;
           const std::string p0 = cur[v], p1 = cur[v | B], l0 = cur[v | 1], l1 = cur[v | 1 | B];
-          o << "        " << acc << " += grad_term<" << G << ">(" << p0 << ", " << p1 << ", " << l0 << ", " << l1 << ");\n";
+          o << "        " << acc << " += grad_term<" << (int)od.perm << ">(" << p0 << ", " << p1 << ", " << l0 << ", " << l1 << ");\n";
           const std::string a = g.fresh(), b = g.fresh(), c = g.fresh(), d2 = g.fresh();
           o << "        double2 " << a << ", " << b << ", " << c << ", " << d2 << ";\n";
           o << "        unrotate<" << G << ">(" << p0 << ", " << p1 << ", " << a << ", " << b << ", " << u0 << ", " << u1 << ", "

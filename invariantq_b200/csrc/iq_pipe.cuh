@@ -172,21 +172,41 @@ __device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
 // Adjoint step on slot 0 (psi / lambda select bit) and slot B (the qubit):
 // returns this thread's share of Im<lambda| P |psi> for generator P (GEN 0 = X,
 // 1 = Y, 2 = Z), then un-applies the rotation exp(-i t P / 2) on the qubit in
-// both halves.  m is the inverse rotation, used through its structure:
-// GEN 0: [[c, i s], [i s, c]]; GEN 1: [[c, s], [-s, c]] (real);
-// GEN 2: diag(e^{i t/2}, e^{-i t/2}).  Inputs are read before outputs are
-// written (in-place safe).
-template <int GEN>
+// both halves.  m is the inverse rotation or a multiple of it, used through
+// its structure (FORM, a GradForm): GEN 0: [[c, i s], [i s, c]], [[1, i t],
+// [i t, 1]] or [[u, i], [i, u]]; GEN 1: [[c, s], [-s, c]], [[1, t], [-t, 1]] or
+// [[u, 1], [-1, u]]; GEN 2: diag(e^{i t/2}, e^{-i t/2}) or diag(1, u3).
+// Inputs are read before outputs are written (in-place safe).
+template <int GEN, int FORM = 0>
 __device__ __forceinline__ void unrotate(double2 x0, double2 x1, double2& y0, double2& y1, double2 u0, double2 u1,
                                          double2 u3) {
-  if (GEN == 0) {         // y0 = c x0 + i s x1, y1 = i s x0 + c x1
+  if (GEN == 0 && FORM == 1) {          // y0 = x0 + i t x1, y1 = x1 + i t x0
+    const double t = u1.y;
+    y0 = make_double2(fma(-t, x1.y, x0.x), fma(t, x1.x, x0.y));
+    y1 = make_double2(fma(-t, x0.y, x1.x), fma(t, x0.x, x1.y));
+  } else if (GEN == 0 && FORM == 2) {   // y0 = u x0 + i x1, y1 = u x1 + i x0
+    const double u = u0.x;
+    y0 = make_double2(fma(u, x0.x, -x1.y), fma(u, x0.y, x1.x));
+    y1 = make_double2(fma(u, x1.x, -x0.y), fma(u, x1.y, x0.x));
+  } else if (GEN == 0) {         // y0 = c x0 + i s x1, y1 = i s x0 + c x1
     const double c = u0.x, sn = u1.y;
     y0 = make_double2(fma(c, x0.x, -sn * x1.y), fma(c, x0.y, sn * x1.x));
     y1 = make_double2(fma(c, x1.x, -sn * x0.y), fma(c, x1.y, sn * x0.x));
+  } else if (GEN == 1 && FORM == 1) {   // y0 = x0 + t x1, y1 = x1 - t x0
+    const double t = u1.x;
+    y0 = make_double2(fma(t, x1.x, x0.x), fma(t, x1.y, x0.y));
+    y1 = make_double2(fma(-t, x0.x, x1.x), fma(-t, x0.y, x1.y));
+  } else if (GEN == 1 && FORM == 2) {   // y0 = u x0 + x1, y1 = u x1 - x0
+    const double u = u0.x;
+    y0 = make_double2(fma(u, x0.x, x1.x), fma(u, x0.y, x1.y));
+    y1 = make_double2(fma(u, x1.x, -x0.x), fma(u, x1.y, -x0.y));
   } else if (GEN == 1) {  // y0 = c x0 + s x1, y1 = c x1 - s x0
     const double c = u0.x, sn = u1.x;
     y0 = make_double2(fma(c, x0.x, sn * x1.x), fma(c, x0.y, sn * x1.y));
     y1 = make_double2(fma(c, x1.x, -sn * x0.x), fma(c, x1.y, -sn * x0.y));
+  } else if (FORM == 1) { // diag(1, u3)
+    y0 = x0;
+    y1 = cmul(u3, x1);
   } else {                // diagonal phases
     y0 = cmul(u0, x0);
     y1 = cmul(u3, x1);

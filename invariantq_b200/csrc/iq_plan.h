@@ -69,8 +69,9 @@ enum OpKind : uint8_t {
   OP_GRAD2 = 8, // adjoint step on slots a (psi/lambda select bit) and b (qubit bit): add
                 // Im<lambda|P|psi> (P = X, Y, Z for `perm` = 0, 1, 2) to gradient term
                 // `gidx`, then apply the 2x2 matrix at `mat` to the qubit for both halves; the
-                // matrix is the inverse rotation exp(+i t P / 2) and is read through its
-                // structure (entries 0, 1, 3)
+                // matrix is the inverse rotation exp(+i t P / 2), or a multiple of it, read
+                // through its structure (entries 0, 1, 3) in the form `flags` names:
+                // GRAD_PLAIN, GRAD_TAN, GRAD_COT (X, Y) or GRAD_PHASE (Z)
   OP_N1R = 9,   // one-qubit 2x2 on register slot a whose row-0 entry in column `perm`
                 // (0 or 1) is exactly 1: that product is skipped (6 instead of 8 FMAs per
                 // amplitude); the matrix is stored whole, so a lane placement runs it as OP_D1L
@@ -83,6 +84,18 @@ enum OpKind : uint8_t {
 
 // flags
 constexpr uint8_t OPF_UNIT_PHASE = 1;  // monomial whose phases are all exactly 1
+
+// Forms of an adjoint step's inverse rotation (OP_GRAD2 flags).  The step may
+// apply a multiple of the inverse: a unit phase common to psi and lambda
+// leaves every later Im<lambda|P|psi> unchanged; a real factor k scales
+// every later term by k^2, which the host divides out (ansatz_backward's
+// grad_scale).
+enum GradForm : uint8_t {
+  GRAD_PLAIN = 0,   // [[c, i s], [i s, c]] (X), [[c, s], [-s, c]] (Y), diag(u0, u3) (Z)
+  GRAD_TAN = 1,     // X, Y divided by c: [[1, i t], [i t, 1]], [[1, t], [-t, 1]] (t = Im / Re m[1])
+  GRAD_COT = 2,     // X, Y divided by s: [[u, i], [i, u]], [[u, 1], [-1, u]] (u = Re m[0])
+  GRAD_PHASE = 1,   // Z divided by its row-0 phase: diag(1, u3)
+};
 
 struct OpDesc {          // 16 bytes
   uint8_t kind;
@@ -144,11 +157,16 @@ struct SchedOp {
   uint32_t mat;          // complex offset of the 2^k x 2^k row-major matrix (dense) or 2^k phases (monomial)
   uint32_t dense;        // complex offset of the dense 2^k x 2^k matrix (always present)
   uint8_t norm;          // k = 1 dense, normalised: row-0 entry in column norm - 1 is exactly 1 (0: not)
-  uint8_t rot;           // k = 1 real rotation, normalised: 1 = tan form, 2 = cot form (0: not)
+  uint8_t rot;           // k = 1 real rotation, normalised: 1 = tan form, 2 = cot form (0: not);
+                         // adjoint step: its inverse rotation's form (OpDesc::flags of OP_GRAD2)
   uint8_t urows;         // monomial: bit r = row r's phase is exactly 1
   uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
   uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
   uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
+  // factor the operation multiplies the scale of a scaled backward sweep by
+  // (stored amplitudes = true amplitudes / scale; 0 means 1): a scaled
+  // adjoint step's divisor, or 1 / f for a scalar operation multiplying by f
+  double smul;
 };
 
 struct SchedParams {
@@ -163,11 +181,17 @@ struct SchedParams {
 
 // A planned pass.  desc.ops[].mat are offsets into the caller's op matrix pool
 // (SchedOp::mat), so the pool uploaded once per flush serves every pass.
+#if !defined(__CUDACC_RTC__)
+}  // namespace iqb
+#include <vector>
+namespace iqb {
 struct PassPlan {
   PassDesc desc;
   int nsrc;              // number of scheduled ops
   double cost;           // planned arithmetic cost per amplitude
+  std::vector<uint32_t> src;   // index of desc.ops[i]'s operation in the scheduled list
 };
+#endif
 
 // Cost (real multiply-adds per amplitude) of applying an operation in a pass.
 double op_cost(const SchedOp& op);
@@ -399,8 +423,37 @@ void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* param
 // lambda = H psi (1), bit q + 1 is qubit q): for every gate from last to first,
 // an adjoint step (gradient term + inverse rotation) per rotation angle, or the
 // inverse of a fixed gate.  grad_param[t] is the parameter gradient term t adds to.
+// Z steps apply the phase-free form (GRAD_PHASE: no scale).  With `scaled`,
+// X and Y steps apply the tan or cot form, dividing by the larger of |c| and
+// |s|, and grad_scale[t] is the factor term t's accumulated value must be
+// multiplied by (the square of the product of the divisors applied before
+// it; 1 without `scaled`); a scalar operation restores the true scale
+// whenever that product leaves [2^-64, 2^64].  The forms then depend on the
+// angles, so `scaled` suits a parameter set that shares its plans with no other.
 void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit = 0);
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit = 0,
+                     bool scaled = false, std::vector<double>* grad_scale = nullptr);
+// One parameter set's operation lists as the adjoint executor runs them.
+// single_set: the forward goes through decompose_one_qubit_ops and
+// normalize_one_qubit_ops (two-qubit monomials kept apart) and the backward
+// is `scaled` -- structures that depend on the angles, for a set whose plans
+// serve no other set; otherwise (fuse) runs of one- and two-qubit gates are
+// fused into 4x4 blocks, a structure every set of the circuit shares.
+struct AdjointOps {
+  std::vector<SchedOp> fw, bw;
+  std::vector<cplx64> fpool, bpool;
+  std::vector<int> grad_param;
+  std::vector<double> grad_scale;
+};
+void adjoint_ops(int n, const std::vector<AnsatzOp>& ops, const double* params, bool backward, bool fuse,
+                 bool single_set, AdjointOps& j);
+// The scale factors of a backward sweep's gradient terms in the order the
+// operations run: the planner moves adjoint steps on different qubits past
+// each other, so the scale each term sees is the product of the factors
+// (SchedOp::smul) of the operations that run before it.  `plans` are the
+// passes planned from `ops` (null: the operations run in list order); scale
+// receives, per gradient term, the square of the scale it is accumulated at.
+void exec_grad_scales(const std::vector<PassPlan>* plans, const std::vector<SchedOp>& ops, std::vector<double>& scale);
 // Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
 // and fills perm/phases/unit if every row and column holds exactly one nonzero.
 int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);

@@ -451,6 +451,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
       sd.op0 = (uint16_t)nout;
       for (int i : s.ops) {
         const SchedOp& o = ops[i];
+        plan.src.push_back((uint32_t)i);
         OpDesc& od = d.ops[nout++];
         od.k = o.k;
         od.mat = o.mat;
@@ -479,7 +480,7 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
           od.b = (uint8_t)slot_of[j1];
           if (o.grad) {
             od.perm = o.gen;
-            od.flags = 0;
+            od.flags = o.rot;                  // the inverse rotation's form (GradForm)
             od.gidx = d.ngrad;                 // local index; the global term goes to grad_term
             d.grad_term[d.ngrad++] = o.gidx;
           }
@@ -567,7 +568,8 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
     const SchedOp& o = ops[i];
     // wide blocks and adjoint steps pass through unchanged, and so do two-qubit
     // monomials (CX, CZ, SWAP) when they are cheaper alone than inside a 4x4
-    if (o.k >= 3 || o.grad || (monomial_barrier && o.k == 2 && o.mono)) {
+    // adjoint steps and the scalars of a scaled backward sweep (smul) keep their place unchanged
+    if (o.k >= 3 || o.grad || o.smul != 0.0 || (monomial_barrier && o.k == 2 && o.mono)) {
       for (int j = 0; j < o.k; ++j) { open[o.q[j]] = -1; last[o.q[j]] = (int)blocks.size(); }
       Block b;
       b.k = 0;
@@ -1048,29 +1050,68 @@ void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* param
 }
 
 void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit) {
+                     std::vector<cplx64>& pool, std::vector<int>& grad_param, int select_bit, bool scaled,
+                     std::vector<double>* grad_scale) {
   if (select_bit < 0) select_bit = n;
   auto bit = [&](int q) { return q + (q >= select_bit ? 1 : 0); };   // index bit of qubit q in the joint array
+  double sigma = 1.0;   // stored amplitudes = true amplitudes / sigma
   for (size_t i = ops.size(); i-- > 0;) {
     const AnsatzOp& o = ops[i];
     int gen[3], par[3];
     const int nr = rotations_of(o, gen, par);
     if (nr) {
       for (int r = nr - 1; r >= 0; --r) {   // last rotation of the gate first
-        cdd m[4], md[4];
-        rotation(gen[r], params[par[r]], m);
-        dagger2(m, md);
+        const double th = params[par[r]];
+        cdd md[4];
+        uint8_t form = GRAD_PLAIN;
+        double kappa = 1.0;
+        if (gen[r] == 2) {
+          // exp(+i th Z / 2) divided by its row-0 phase: diag(1, e^{-i th})
+          form = GRAD_PHASE;
+          md[0] = 1.0; md[1] = 0.0; md[2] = 0.0; md[3] = cdd(std::cos(th), -std::sin(th));
+        } else if (scaled) {
+          const double c = std::cos(th / 2.0), s = std::sin(th / 2.0);
+          const cdd j = gen[r] == 0 ? cdd(0.0, 1.0) : cdd(1.0, 0.0);   // X: i s off the diagonal; Y: +s, -s
+          const cdd jl = gen[r] == 0 ? cdd(0.0, 1.0) : cdd(-1.0, 0.0);
+          if (std::fabs(c) >= std::fabs(s)) {
+            form = GRAD_TAN;
+            kappa = c;
+            const double t = s / c;
+            md[0] = 1.0; md[1] = j * t; md[2] = jl * t; md[3] = 1.0;
+          } else {
+            form = GRAD_COT;
+            kappa = s;
+            const double u = c / s;
+            md[0] = u; md[1] = j; md[2] = jl; md[3] = u;
+          }
+        } else {
+          cdd m[4];
+          rotation(gen[r], th, m);
+          dagger2(m, md);
+        }
         SchedOp g{};
         g.k = 2;
         g.q[0] = (uint8_t)select_bit;     // psi / lambda select bit
         g.q[1] = (uint8_t)bit(o.q0);
         g.grad = 1;
         g.gen = (uint8_t)gen[r];
+        g.rot = form;
         g.gidx = (uint32_t)grad_param.size();
         g.dense = g.mat = (uint32_t)pool.size();
         for (int j = 0; j < 4; ++j) pool.push_back({md[j].real(), md[j].imag()});
+        g.smul = kappa;
         out.push_back(g);
         grad_param.push_back(par[r]);
+        if (grad_scale) grad_scale->push_back(sigma * sigma);
+        sigma *= kappa;
+        if (std::fabs(sigma) < 0x1p-64 || std::fabs(sigma) > 0x1p64) {
+          // back to the true scale: every amplitude of both halves times sigma
+          const cdd sc[4] = {sigma, 0.0, 0.0, sigma};
+          const int q[1] = {bit(o.q0)};
+          push_op(out, pool, 1, q, sc);
+          out.back().smul = 1.0 / sigma;
+          sigma = 1.0;
+        }
       }
       continue;
     }
@@ -1083,6 +1124,42 @@ void ansatz_backward(int n, const std::vector<AnsatzOp>& ops, const double* para
     int qj[2] = {bit(q[0]), k > 1 ? bit(q[1]) : 0};
     push_op(out, pool, k, qj, md);
   }
+}
+
+void adjoint_ops(int n, const std::vector<AnsatzOp>& ops, const double* params, bool backward, bool fuse,
+                 bool single_set, AdjointOps& j) {
+  j.fw.clear(); j.bw.clear(); j.fpool.clear(); j.bpool.clear(); j.grad_param.clear(); j.grad_scale.clear();
+  std::vector<SchedOp> raw;
+  ansatz_forward(n, ops, params, raw, j.fpool);
+  if (single_set) {
+    j.fw = fuse_two_qubit_blocks(raw, j.fpool, true);
+    decompose_one_qubit_ops(j.fw, j.fpool);
+    normalize_one_qubit_ops(j.fw, j.fpool);
+  } else {
+    j.fw = fuse ? fuse_two_qubit_blocks(raw, j.fpool) : raw;
+  }
+  if (!backward) return;
+  raw.clear();
+  ansatz_backward(n, ops, params, raw, j.bpool, j.grad_param, n, single_set, &j.grad_scale);   // [psi | lambda]
+  j.bw = fuse ? fuse_two_qubit_blocks(raw, j.bpool, single_set) : raw;
+}
+
+void exec_grad_scales(const std::vector<PassPlan>* plans, const std::vector<SchedOp>& ops, std::vector<double>& scale) {
+  uint32_t nterms = 0;
+  for (const SchedOp& o : ops)
+    if (o.grad) nterms = std::max(nterms, o.gidx + 1);
+  scale.assign(nterms, 1.0);
+  double sigma = 1.0;
+  auto visit = [&](const SchedOp& o) {
+    if (o.grad) scale[o.gidx] = sigma * sigma;
+    if (o.smul != 0.0) sigma *= o.smul;
+  };
+  if (!plans) {
+    for (const SchedOp& o : ops) visit(o);
+    return;
+  }
+  for (const PassPlan& pl : *plans)
+    for (uint32_t i : pl.src) visit(ops[i]);
 }
 
 void pack_pass_matrices(std::vector<PassPlan>& plans, const cplx64* pool, std::vector<cplx64>& packed) {

@@ -321,7 +321,7 @@ __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
-template <int R, int B, int GEN>
+template <int R, int B, int GEN, int FORM>
 __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
   const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u3 = ld_mat(m, 3);
   double acc = 0.0;
@@ -330,8 +330,8 @@ __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)
     if (v & (1 | (1 << B))) continue;
     const double2 p0 = s[v], p1 = s[v | (1 << B)], l0 = s[v | 1], l1 = s[v | 1 | (1 << B)];
     acc += grad_term<GEN>(p0, p1, l0, l1);
-    unrotate<GEN>(p0, p1, d[v], d[v | (1 << B)], u0, u1, u3);
-    unrotate<GEN>(l0, l1, d[v | 1], d[v | 1 | (1 << B)], u0, u1, u3);
+    unrotate<GEN, FORM>(p0, p1, d[v], d[v | (1 << B)], u0, u1, u3);
+    unrotate<GEN, FORM>(l0, l1, d[v | 1], d[v | 1 | (1 << B)], u0, u1, u3);
   }
   return acc;
 }
@@ -422,12 +422,12 @@ __device__ __forceinline__ void disp_dkr(int k, const double2 (&a)[1 << R], cons
   }
 }
 
-template <int R, int GEN, int B = 1>
+template <int R, int GEN, int FORM, int B = 1>
 __device__ __forceinline__ double disp_grad2_b(int sb, const double2 (&s)[1 << R], double2 (&d)[1 << R],
                                                const double2* m) {
   if constexpr (B < R) {
-    if (sb == B) return grad2<R, B, GEN>(s, d, m);
-    return disp_grad2_b<R, GEN, B + 1>(sb, s, d, m);
+    if (sb == B) return grad2<R, B, GEN, FORM>(s, d, m);
+    return disp_grad2_b<R, GEN, FORM, B + 1>(sb, s, d, m);
   }
   return 0.0;
 }
@@ -445,9 +445,17 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
     case OP_GRAD2: {
       // the planner puts the select bit in slot 0
       double acc;
-      if (od.perm == 0) acc = disp_grad2_b<R, 0>(od.b, s, d, m);
-      else if (od.perm == 1) acc = disp_grad2_b<R, 1>(od.b, s, d, m);
-      else acc = disp_grad2_b<R, 2>(od.b, s, d, m);
+      // generator (perm) and the inverse rotation's form (flags, a GradForm)
+      switch (od.perm * 4 + od.flags) {
+        case 0: acc = disp_grad2_b<R, 0, 0>(od.b, s, d, m); break;
+        case 1: acc = disp_grad2_b<R, 0, 1>(od.b, s, d, m); break;
+        case 2: acc = disp_grad2_b<R, 0, 2>(od.b, s, d, m); break;
+        case 4: acc = disp_grad2_b<R, 1, 0>(od.b, s, d, m); break;
+        case 5: acc = disp_grad2_b<R, 1, 1>(od.b, s, d, m); break;
+        case 6: acc = disp_grad2_b<R, 1, 2>(od.b, s, d, m); break;
+        case 9: acc = disp_grad2_b<R, 2, 1>(od.b, s, d, m); break;
+        default: acc = disp_grad2_b<R, 2, 0>(od.b, s, d, m); break;
+      }
       grad_accumulate(acc, sgrad + od.gidx, lane8, omask);
       break;
     }

@@ -226,7 +226,8 @@ struct Emu {
 // gap != 0: the operations act on the lower half (address bit `gap` = 0) of a
 // state of gap + 1 bits, through passes planned for `gap` bits (PassDesc::gap)
 int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stages, double budget, int fuse,
-             int* npasses, int* ops_per_pass, char* errbuf, int errlen, int gap = 0) {
+             int* npasses, int* ops_per_pass, char* errbuf, int errlen, int gap = 0,
+             std::vector<PassPlan>* plans_out = nullptr) {
   if (fuse) {
     std::vector<cplx64> cp(reinterpret_cast<const cplx64*>(e.pool.data()),
                            reinterpret_cast<const cplx64*>(e.pool.data()) + e.pool.size());
@@ -280,6 +281,7 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
       return -1;
     }
   }
+  if (plans_out) *plans_out = std::move(plans);
   return 0;
 }
 
@@ -289,10 +291,13 @@ int run_plan(Emu& e, std::vector<SchedOp> ops, int M, int c, int R, int max_stag
 // passes exactly as the GPU path does (forward on psi, lambda = H psi, joint
 // array, backward sweep with adjoint steps).  H = sum_t coeffs[t] paulis[t]
 // (n characters per term, character q acting on qubit q).
-extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
-                           const double* params, int nterms, const double* coeffs, const char* paulis, int M, int c,
-                           int R, int max_stages, double budget, double* energy, double* grad, int nparams,
-                           char* errbuf, int errlen) {
+// single_set: the operation lists of a circuit with one parameter set (the
+// forward decomposed into rotations and phases, scaled adjoint steps whose
+// scales are undone in the order the planned passes run them).
+extern "C" int emu_adjoint_forms(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
+                                 const double* params, int nterms, const double* coeffs, const char* paulis, int M,
+                                 int c, int R, int max_stages, double budget, double* energy, double* grad,
+                                 int nparams, int single_set, char* errbuf, int errlen) {
   std::vector<AnsatzOp> ops(nops);
   for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
   std::string err;
@@ -307,15 +312,16 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
   std::vector<cd> psi((size_t)1 << n, 0.0);
   psi[0] = 1.0;
   Emu f;
-  std::vector<SchedOp> fw;
-  std::vector<cplx64> pool;
-  ansatz_forward(n, ops, params, fw, pool);
-  f.pool.assign(reinterpret_cast<const cd*>(pool.data()), reinterpret_cast<const cd*>(pool.data()) + pool.size());
+  AdjointOps jo;   // the executor's operation lists (fused, or the single-set forms)
+  adjoint_ops(n, ops, params, true, true, single_set != 0, jo);
+  const std::vector<SchedOp>& fw = jo.fw;
+  f.pool.assign(reinterpret_cast<const cd*>(jo.fpool.data()),
+                reinterpret_cast<const cd*>(jo.fpool.data()) + jo.fpool.size());
   if (n >= 7) {   // passes planned for n bits with the select bit as their gap
     joint[0] = 1.0;
     f.nbits = n + 1;
     f.state = joint.data();
-    if (run_plan(f, fw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen, n) < 0) return -1;
+    if (run_plan(f, fw, M, c, R, max_stages, budget, 0, nullptr, nullptr, errbuf, errlen, n) < 0) return -1;
     for (uint64_t x = 0; x < (1ULL << n); ++x) psi[x] = joint[x];
   } else {   // the runtime's one-operation kernel: dense matrix, LSB-first qubit list
     for (const SchedOp& o : fw) {
@@ -367,16 +373,29 @@ extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, con
   b.nbits = nj;   // small circuits: zero-padded high bits the gates never touch
   for (uint64_t x = 0; x < dim; ++x) { joint[x] = psi[x]; joint[dim + x] = lam[x]; }
   b.state = joint.data();
-  std::vector<SchedOp> bw;
-  std::vector<cplx64> bpool;
-  std::vector<int> gp;
-  ansatz_backward(n, ops, params, bw, bpool, gp, n);
-  b.pool.assign(reinterpret_cast<const cd*>(bpool.data()), reinterpret_cast<const cd*>(bpool.data()) + bpool.size());
+  const std::vector<int>& gp = jo.grad_param;
+  b.pool.assign(reinterpret_cast<const cd*>(jo.bpool.data()),
+                reinterpret_cast<const cd*>(jo.bpool.data()) + jo.bpool.size());
   b.grads.assign(gp.size(), 0.0);
-  if (run_plan(b, bw, M, c, R, max_stages, budget, 1, nullptr, nullptr, errbuf, errlen) < 0) return -1;
+  std::vector<PassPlan> plans;
+  if (run_plan(b, jo.bw, M, c, R, max_stages, budget, 0, nullptr, nullptr, errbuf, errlen, 0, &plans) < 0) return -1;
+  std::vector<double> scale;
+  exec_grad_scales(&plans, jo.bw, scale);
+  if (scale.size() != gp.size()) {
+    snprintf(errbuf, errlen, "gradient scales: %zu for %zu terms", scale.size(), gp.size());
+    return -1;
+  }
   for (int p = 0; p < nparams; ++p) grad[p] = 0.0;
-  for (size_t t = 0; t < gp.size(); ++t) grad[gp[t]] += b.grads[t];
+  for (size_t t = 0; t < gp.size(); ++t) grad[gp[t]] += b.grads[t] * scale[t];
   return 0;
+}
+
+extern "C" int emu_adjoint(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
+                           const double* params, int nterms, const double* coeffs, const char* paulis, int M, int c,
+                           int R, int max_stages, double budget, double* energy, double* grad, int nparams,
+                           char* errbuf, int errlen) {
+  return emu_adjoint_forms(n, nops, kinds, q0, q1, pidx, params, nterms, coeffs, paulis, M, c, R, max_stages, budget,
+                           energy, grad, nparams, 0, errbuf, errlen);
 }
 
 extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double budget, int fuse, int nops,
@@ -542,15 +561,15 @@ extern "C" int emu_adjoint_sources(int n, int nops, const int* kinds, const int*
     return -1;
   }
   int count = 0;
-  for (int pass = 0; pass < 2; ++pass) {
-    std::vector<SchedOp> raw;
-    std::vector<cplx64> pool;
-    std::vector<int> gp;
-    if (pass == 0) ansatz_forward(n, ops, params, raw, pool);
-    else ansatz_backward(n, ops, params, raw, pool, gp, n);
-    const std::vector<SchedOp> fused = fuse_two_qubit_blocks(raw, pool);
+  // passes 0, 1: forward and backward as a shared plan runs them (fused
+  // blocks); 2, 3: the single-set forms (rotations and phases, scaled steps)
+  for (int pass = 0; pass < 4; ++pass) {
+    AdjointOps jo;
+    adjoint_ops(n, ops, params, true, true, pass >= 2, jo);
+    const std::vector<SchedOp>& fused = (pass & 1) ? jo.bw : jo.fw;
+    std::vector<cplx64>& pool = (pass & 1) ? jo.bpool : jo.fpool;
     SchedParams p{};
-    p.nbits = pass == 0 ? n : n + 1;
+    p.nbits = (pass & 1) ? n + 1 : n;
     if (p.nbits < 7) continue;
     p.M = M;
     p.c = c;

@@ -84,11 +84,13 @@ def test_large_gradient_vs_gpu_parameter_shift(G, n, layers):
     assert np.max(np.abs(g - G.parameter_shift_gradient(a, h, th))) < PS_TOL
 
 
-def test_batch_matches_single_jobs(G):
+def test_batch_matches_single_jobs(G, monkeypatch):
     """Uneven circuits, several parameter sets each (run together in one launch
     per pass), on several streams: bit-identical for any number of streams (fixed
-    reduction order), equal to one set at a time within 1e-13 (the sets' tiles
-    meet the CTAs in another order), and to the parameter shift within 1e-9."""
+    reduction order); equal to one set at a time within 1e-13 through the same
+    operation forms (the sets' tiles meet the CTAs in another order) and within
+    1e-12 through the single-set forms (rotations and phases, scaled adjoint
+    steps: other roundings); to the parameter shift within 1e-9."""
     rng = np.random.default_rng(9)
     jobs = []
     for n, L in [(4, 2), (10, 3), (13, 2), (7, 4), (12, 1)]:
@@ -103,8 +105,13 @@ def test_batch_matches_single_jobs(G):
     for (a, h, P), (e, g) in zip(jobs, out):
         for s in range(P.shape[0]):
             e1, g1 = G.adjoint_gradient(a, h, P[s])
-            assert e[s] == e1
-            assert np.max(np.abs(g[s] - g1)) < 1e-13
+            assert abs(e[s] - e1) < 1e-12 and np.max(np.abs(g[s] - g1)) < 1e-12
+            assert np.max(np.abs(g1 - G.parameter_shift_gradient(a, h, P[s]))) < PS_TOL
+            monkeypatch.setenv("IQ_ADJOINT_SINGLE_FORMS", "0")
+            e0, g0 = G.adjoint_gradient(a, h, P[s])
+            monkeypatch.delenv("IQ_ADJOINT_SINGLE_FORMS")
+            assert e[s] == e0
+            assert np.max(np.abs(g[s] - g0)) < 1e-13
             assert np.max(np.abs(g[s] - G.parameter_shift_gradient(a, h, P[s]))) < PS_TOL
 
 

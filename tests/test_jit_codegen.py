@@ -136,7 +136,11 @@ def test_adjoint_kernels_compile(emu, narrow):
     assert rc > 0, text
     srcs = text.split("\n//@@PASS@@\n")
     assert all(("narrow=1" in s) == bool(narrow) for s in srcs)
-    for s in (srcs[0], max(srcs, key=len)):
+    # every adjoint-step form: phase-free Z steps, and the single-set plans'
+    # tan / cot Y steps
+    forms = ["unrotate<2, 1>", "unrotate<1, 1>", "unrotate<1, 2>"]
+    picked = [next(s for s in srcs if f in s) for f in forms]
+    for s in [srcs[0], max(srcs, key=len)] + picked:
         rc, log, size = compile_nvrtc(lib, s)
         assert rc == 0, log[:3000]
         assert size > 0
