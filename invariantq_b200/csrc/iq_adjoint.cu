@@ -824,6 +824,13 @@ int run_batch(std::vector<std::unique_ptr<Circuit>>& circs, int nstreams, bool w
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   Cfg cfg = Cfg::from_env();
   cfg.c64 = c64;
+  if (c64) {
+    // complex64 passes keep a float2 tile (32 KiB at 2^12 amplitudes): four
+    // CTAs fit per SM, whose extra warps hide the direct global loads (30
+    // qubits: 1.99 s against 2.13 s with three)
+    cfg.sp.M = env_int("IQ_C64_TILE_BITS", cfg.sp.M);
+    cfg.tl.ctas_per_sm = env_int("IQ_C64_CTAS_PER_SM", 4);
+  }
   // jobs: a circuit's parameter sets in groups whose joint arrays ([psi |
   // lambda], 32 B x 2^n per set) fit the per-job budget; the energy-only path
   // (the plain baseline) runs one set per job on a state buffer (16 B x 2^n)

@@ -481,7 +481,8 @@ cudaError_t jit_launch_narrow(const JitKernel* kc, const PassDesc& d, const doub
   if (!k->narrow) return cudaErrorInvalidValue;
   if (d.ngrad && !grad_partials) return cudaErrorInvalidValue;
   const Driver& dr = driver();
-  const size_t smem = 1024 + ((size_t)16 << d.M) + (size_t)d.mat_elems * 16 + (size_t)d.ngrad * (k->nt / 8) * 8;
+  // [float2 tile][matrix block][gradient accumulators] (direct_set_pass)
+  const size_t smem = 1024 + ((size_t)8 << d.M) + (size_t)d.mat_elems * 16 + (size_t)d.ngrad * (k->nt / 8) * 8;
   if (!k->smem_limit_set.load(std::memory_order_acquire)) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);

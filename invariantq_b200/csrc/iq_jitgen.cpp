@@ -28,11 +28,12 @@ std::string mat(uint32_t i) { return (g_set_mode ? "smat[" : "Mt.m[") + std::to_
 // agree bit for bit.
 // gmode bit 0: the stage loads its registers from the complex64 array in
 // global memory (gst + tile base tb + physical offsets) instead of the tile;
-// bit 1: it stores them there.
+// bit 1: it stores them there; bit 2: the shared-memory tile is complex64
+// (float2 `ftile`: values widened to FP64 on load, rounded once on store).
 bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int gmode = 0) {
   const StageDesc& sd = d.st[s];
   const int R = d.R, NV = 1 << R;
-  const bool gload = gmode & 1, gstore = gmode & 2, use_smem = !(gload && gstore);
+  const bool gload = gmode & 1, gstore = gmode & 2, use_smem = !(gload && gstore), ftile = gmode & 4;
   std::ostringstream& o = g.o;
   uint32_t sb[kMaxK];
   for (int i = 0; i < R; ++i) sb[i] = swz(1u << sd.S[i]);
@@ -69,13 +70,16 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
     const uint32_t k = voffc(v) & 7u;
     if (!ptr[k].empty()) continue;
     ptr[k] = "p" + std::to_string(k);
-    o << "        double2* const " << ptr[k] << " = tile + (base ^ " << k << "u);\n";
+    o << "        " << (ftile ? "float2* const " : "double2* const ") << ptr[k] << " = " << (ftile ? "ftile" : "tile")
+      << " + (base ^ " << k << "u);\n";
   }
   auto at = [&](int v) { return ptr[voffc(v) & 7u] + "[" + std::to_string(voffc(v) & ~7u) + "]"; };
+  auto atp = [&](int v) { return ptr[voffc(v) & 7u] + " + " + std::to_string(voffc(v) & ~7u); };
   std::vector<std::string> cur(NV);
   for (int v = 0; v < NV; ++v) {
     cur[v] = g.fresh();
-    o << "        const double2 " << cur[v] << " = " << (gload ? "ldn(" + goff(v) + ")" : at(v)) << ";\n";
+    o << "        const double2 " << cur[v] << " = "
+      << (gload ? "ldn(" + goff(v) + ")" : (ftile ? "ldn(" + atp(v) + ")" : at(v))) << ";\n";
   }
   auto def = [&](const std::string& expr) {
     const std::string n = g.fresh();
@@ -251,6 +255,7 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
   }
   for (int v = 0; v < NV; ++v) {
     if (gstore) o << "        stn(" << goff(v) << ", " << cur[v] << ");\n";
+    else if (ftile) o << "        stn(" << atp(v) << ", " << cur[v] << ");\n";
     else o << "        " << at(v) << " = " << cur[v] << ";\n";
   }
   o << "      }\n    }\n    __syncthreads();\n";
@@ -315,19 +320,19 @@ std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks,
   const uint32_t nmat = d.mat_elems ? d.mat_elems : 1;
   Gen g;
   std::ostringstream& o = g.o;
-  o << "// generated by iq_jitgen (iq-jit-1): NT=" << NT << " sets=" << (set_mode ? 1 : 0)
+  o << "// generated by iq_jitgen (iq-jit-2): NT=" << NT << " sets=" << (set_mode ? 1 : 0)
     << " narrow=" << (narrow ? 1 : 0) << " M=" << (int)d.M
     << " c=" << (int)d.c << " R=" << (int)d.R
     << " stages=" << (int)d.nstages << " ops=" << d.nops << "\n";
   o << "#include \"iq_pipe.cuh\"\nusing namespace iqb;\n";
   if (narrow) {
     o << "struct JitStages {\n  const PassDesc& P;\n  float2* gst;\n  int lane8, octet;\n  unsigned omask;\n";
-    o << "  __device__ __forceinline__ void operator()(double2* tile, const double2* smat, double* gslots, "
+    o << "  __device__ __forceinline__ void operator()(float2* ftile, const double2* smat, double* gslots, "
          "unsigned long long t) {\n";
     o << "    const unsigned long long tb = tile_base(t, P);\n";
-    o << "    double* const gs = gslots + octet * " << d.ngrad << ";\n    (void)gs; (void)tile;\n";
+    o << "    double* const gs = gslots + octet * " << d.ngrad << ";\n    (void)gs; (void)ftile;\n";
     for (int s = 0; s < d.nstages; ++s) {
-      const int gm = (s == 0 ? 1 : 0) | (s == d.nstages - 1 ? 2 : 0);
+      const int gm = (s == 0 ? 1 : 0) | (s == d.nstages - 1 ? 2 : 0) | 4;
       if (!gen_stage(g, d, s, NT, err, gm)) return "";
     }
     o << "  }\n};\n";

@@ -446,9 +446,10 @@ __device__ __forceinline__ void set_tile_pass(const CUtensorMap& tm, const PassD
 
 // ---- passes over complex64 (float2) arrays: the first stage loads its
 // registers straight from global memory (widened to FP64), the last stage
-// stores them there (rounded once to FP32), and the stages between exchange
-// through a shared-memory tile of double2 as in the TMA pipeline.  Every CTA
-// walks its tiles (blockIdx.x, + gridDim.x, ...); no asynchronous copies.
+// stores them there (rounded to FP32), and the stages between exchange
+// through a shared-memory tile of float2 (each stage boundary rounds to FP32
+// as the array does; all arithmetic is FP64).  Every CTA walks its tiles
+// (blockIdx.x, + gridDim.x, ...); no asynchronous copies.
 
 // Physical index bits of tile-local index L: bits below c are themselves, bit
 // c + i is H[i].
@@ -466,15 +467,16 @@ __device__ __forceinline__ void stn(float2* p, double2 v) {
   *p = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
 }
 
-// Dynamic shared memory: [one double2 tile][the current set's matrix block]
-// [gradient accumulators: one row of ngrad per octet].  stages(tile, smat,
-// gslots, t) runs the pass's stages on tile t (each stage ends with a
-// __syncthreads()).  Set switches as in SetTileBody.
+// Dynamic shared memory: [one float2 tile of 2^M elements][the current set's
+// matrix block][gradient accumulators: one row of ngrad per octet].
+// stages(tile, smat, gslots, t) runs the pass's stages on tile t (each stage
+// ends with a __syncthreads()).  Set switches as in SetTileBody.
 template <int NT, class Stages>
 __device__ __forceinline__ void direct_set_pass(const PassDesc& P, const double2* mats, double* grad_partials,
                                                 unsigned char* smem_raw, Stages& stages) {
-  double2* tile = aligned_tiles(smem_raw);
-  double2* smat = tile + (1u << P.M);
+  double2* const tiles = aligned_tiles(smem_raw);
+  float2* tile = reinterpret_cast<float2*>(tiles);
+  double2* smat = tiles + (1u << (P.M - 1));   // after the tile's 8 << M bytes
   double* gslots = reinterpret_cast<double*>(smat + P.mat_elems);
   const int tid = threadIdx.x;
   const uint32_t sshift = (P.nsets > 1) ? P.set_shift : 63u;
