@@ -209,6 +209,25 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
         }
         break;
       }
+      case OP_X2R: {   // channel-shaped 4x4: corners mix x0 / x3, the middle scales x1, x2
+        const int A = 1 << od.a, B = 1 << od.b;
+        const std::string tmpl = std::string("xpat4<") + ((od.flags & 1) ? "true" : "false") + ", " +
+                                 ((od.flags & 2) ? "true" : "false") + ">";
+        const std::string mv = g.fresh();
+        o << "        const double2 " << mv << "[6] = {" << mat(m + 0) << ", " << mat(m + 3) << ", " << mat(m + 12)
+          << ", " << mat(m + 15) << ", " << mat(m + 5) << ", " << mat(m + 10) << "};\n";
+        for (int v = 0; v < NV; ++v) {
+          if (v & (A | B)) continue;
+          const std::string x[4] = {g.fresh(), g.fresh(), g.fresh(), g.fresh()};
+          const int idx[4] = {v, v | A, v | B, v | A | B};
+          o << "        double2 " << x[0] << " = " << cur[idx[0]] << ", " << x[1] << " = " << cur[idx[1]] << ", "
+            << x[2] << " = " << cur[idx[2]] << ", " << x[3] << " = " << cur[idx[3]] << ";\n";
+          o << "        " << tmpl << "(" << x[0] << ", " << x[1] << ", " << x[2] << ", " << x[3] << ", " << mv << "[0], "
+            << mv << "[1], " << mv << "[2], " << mv << "[3], " << mv << "[4], " << mv << "[5]);\n";
+          for (int r = 0; r < 4; ++r) cur[idx[r]] = x[r];
+        }
+        break;
+      }
       case OP_DKR: {
         const int D = 1 << od.k;
         if (od.k > R) { err = "dense block wider than the register slots"; return false; }

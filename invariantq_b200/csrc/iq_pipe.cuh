@@ -165,6 +165,32 @@ __device__ __forceinline__ double2 rot_lane(double w, bool hi, double2 x, double
   return make_double2(fma(w, x.x, hi ? p.x : -p.x), fma(w, x.y, hi ? p.y : -p.y));
 }
 
+// OP_X2R on one amplitude quadruple x0..x3 (local index bit 0 = slot a, bit 1
+// = slot b) with the 4x4 m (row-major): corners (0,0), (0,3), (3,0), (3,3) mix
+// x0 and x3, the middle (1,1), (2,2) scales x1 and x2.  CR / MR: the corner /
+// middle entries are real (their imaginary parts are not read).
+template <bool CR, bool MR>
+__device__ __forceinline__ void xpat4(double2& x0, double2& x1, double2& x2, double2& x3, double2 m0, double2 m3,
+                                      double2 m12, double2 m15, double2 m5, double2 m10) {
+  double2 y0, y3;
+  if (CR) {
+    y0 = make_double2(fma(m3.x, x3.x, m0.x * x0.x), fma(m3.x, x3.y, m0.x * x0.y));
+    y3 = make_double2(fma(m15.x, x3.x, m12.x * x0.x), fma(m15.x, x3.y, m12.x * x0.y));
+  } else {
+    y0 = cfma(cmul(m0, x0), m3, x3);
+    y3 = cfma(cmul(m12, x0), m15, x3);
+  }
+  if (MR) {
+    x1 = make_double2(m5.x * x1.x, m5.x * x1.y);
+    x2 = make_double2(m10.x * x2.x, m10.x * x2.y);
+  } else {
+    x1 = cmul(m5, x1);
+    x2 = cmul(m10, x2);
+  }
+  x0 = y0;
+  x3 = y3;
+}
+
 __device__ __forceinline__ double2 shfl_xor2(double2 v, int dl, unsigned mask) {
   return make_double2(__shfl_xor_sync(mask, v.x, dl, 8), __shfl_xor_sync(mask, v.y, dl, 8));
 }

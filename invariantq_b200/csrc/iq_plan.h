@@ -80,7 +80,18 @@ enum OpKind : uint8_t {
                 // stored whole, so a lane placement runs it as OP_D1L
   OP_R1L = 11,  // the same rotation on lane bit a: each lane combines its own amplitude with its
                 // partner's (warp shuffle): 2 FMAs per amplitude in the tan form
+  OP_X2R = 12,  // 4x4 on register slots a (bit 0) and b (bit 1) whose only nonzero entries are
+                // the corners (0,0), (0,3), (3,0), (3,3) and the middle (1,1), (2,2) -- the shape
+                // of the superoperators of depolarizing, amplitude / phase damping and thermal
+                // relaxation channels and of their products; stored whole (16 entries); flags
+                // bit 0: the corners are real, bit 1: the middle is real (3 to 6 FMAs per
+                // amplitude)
 };
+
+// SchedOp::xpat bits (0: not OP_X2R's shape)
+constexpr uint8_t XPAT_SHAPE = 1;
+constexpr uint8_t XPAT_CORNERS_REAL = 2;
+constexpr uint8_t XPAT_MIDDLE_REAL = 4;
 
 // flags
 constexpr uint8_t OPF_UNIT_PHASE = 1;  // monomial whose phases are all exactly 1
@@ -161,6 +172,7 @@ struct SchedOp {
                          // adjoint step: its inverse rotation's form (OpDesc::flags of OP_GRAD2)
   uint8_t urows;         // monomial: bit r = row r's phase is exactly 1
   uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
+  uint8_t xpat;          // k = 2 dense matrix of OP_X2R's shape: XPAT_* bits (0: not)
   uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
   uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
   // factor the operation multiplies the scale of a scaled backward sweep by
@@ -457,5 +469,8 @@ void exec_grad_scales(const std::vector<PassPlan>* plans, const std::vector<Sche
 // Classify a 2^k x 2^k row-major matrix (interleaved re/im doubles): returns 1
 // and fills perm/phases/unit if every row and column holds exactly one nonzero.
 int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uint8_t* unit);
+// OP_X2R's shape for a 4x4 row-major matrix (interleaved re/im doubles):
+// 0 = not that shape, else XPAT_SHAPE plus XPAT_CORNERS_REAL / XPAT_MIDDLE_REAL.
+int classify_xpattern(const double* m);
 }  // namespace iqb
 #endif

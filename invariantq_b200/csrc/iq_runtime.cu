@@ -371,6 +371,8 @@ struct Engine {
         o.unit = unit;
         o.mat = (uint32_t)pool.size();
         for (int i = 0; i < d; ++i) pool.push_back({ph[2 * i], ph[2 * i + 1]});
+      } else if (k == 2) {
+        o.xpat = (uint8_t)classify_xpattern(reinterpret_cast<const double*>(m));
       }
     }
     ops.push_back(o);

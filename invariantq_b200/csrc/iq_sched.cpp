@@ -36,6 +36,7 @@ double op_cost(const SchedOp& op, double grad_cost) {
   }
   if (op.rot) return 2.0;
   if (op.norm) return 6.0;
+  if (op.xpat) return ((op.xpat & XPAT_CORNERS_REAL) ? 2.0 : 4.0) + ((op.xpat & XPAT_MIDDLE_REAL) ? 1.0 : 2.0);
   return 4.0 * double(1u << op.k);
 }
 
@@ -66,6 +67,20 @@ int classify_monomial(const double* m, int k, uint8_t* perm, double* phases, uin
   *perm = p;
   *unit = u;
   return 1;
+}
+
+int classify_xpattern(const double* m) {
+  bool corners_real = true, middle_real = true;
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      const double re = m[2 * (r * 4 + c)], im = m[2 * (r * 4 + c) + 1];
+      const bool corner = (r == 0 || r == 3) && (c == 0 || c == 3);
+      const bool middle = r == c && (r == 1 || r == 2);
+      if (!corner && !middle && (re != 0.0 || im != 0.0)) return 0;
+      if (corner && im != 0.0) corners_real = false;
+      if (middle && im != 0.0) middle_real = false;
+    }
+  return 1 | (corners_real ? XPAT_CORNERS_REAL : 0) | (middle_real ? XPAT_MIDDLE_REAL : 0);
 }
 
 namespace {
@@ -475,7 +490,8 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
         } else if (o.k == 2) {
           const int j0 = pos[o.q[0]], j1 = pos[o.q[1]];
           if (slot_of[j0] < 0 || slot_of[j1] < 0) { err = "internal: 2q operation outside slots"; return -1; }
-          od.kind = o.grad ? OP_GRAD2 : (o.mono ? OP_M2R : OP_D2R);
+          od.kind = o.grad ? OP_GRAD2 : (o.mono ? OP_M2R : (o.xpat ? OP_X2R : OP_D2R));
+          if (od.kind == OP_X2R) od.flags = (uint8_t)(o.xpat >> 1);   // XPAT_* >> 1: bit 0 corners, bit 1 middle real
           od.a = (uint8_t)slot_of[j0];
           od.b = (uint8_t)slot_of[j1];
           if (o.grad) {
@@ -548,6 +564,7 @@ struct Block {
   bool dead = false;
   int src = -1;         // index of the original op when the block is that op unchanged
   bool changed = false;
+  bool xpat = false;    // a run of OP_X2R-shaped operations on one pair, kept apart from one-qubit blocks
 };
 
 }  // namespace
@@ -569,6 +586,36 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
     // wide blocks and adjoint steps pass through unchanged, and so do two-qubit
     // monomials (CX, CZ, SWAP) when they are cheaper alone than inside a 4x4
     // adjoint steps and the scalars of a scaled backward sweep (smul) keep their place unchanged
+    const bool diagonal2 = o.k == 2 && o.mono && o.perm == 0xE4;   // rows read their own column
+    if (monomial_barrier && o.k == 2 && (o.xpat || diagonal2) && !o.grad && o.smul == 0.0) {
+      // channel-shaped operations (OP_X2R's shape; diagonal ones included)
+      // stay out of one-qubit blocks (a unitary inside would make the block
+      // dense); consecutive ones on the same pair multiply into one block of
+      // the same shape.  A run of one operation keeps it unchanged.
+      const int a = o.q[0], bq = o.q[1];
+      const int B = last[a];
+      const cplx64* U = pool.data() + o.dense;
+      M4 Um;
+      for (int j = 0; j < 16; ++j) Um[j] = U[j];
+      if (B >= 0 && B == last[bq] && blocks[B].xpat) {
+        Block& bl = blocks[B];
+        bl.m = mul4(bl.q[0] == a ? Um : swap_bits(Um.data()), bl.m);
+        bl.changed = true;
+        bl.src = -1;
+        continue;
+      }
+      open[a] = open[bq] = -1;
+      last[a] = last[bq] = (int)blocks.size();
+      Block b;
+      b.k = 2;
+      b.q[0] = a;
+      b.q[1] = bq;
+      b.m = Um;
+      b.src = (int)i;
+      b.xpat = true;
+      blocks.push_back(b);
+      continue;
+    }
     if (o.k >= 3 || o.grad || o.smul != 0.0 || (monomial_barrier && o.k == 2 && o.mono)) {
       for (int j = 0; j < o.k; ++j) { open[o.q[j]] = -1; last[o.q[j]] = (int)blocks.size(); }
       Block b;
@@ -688,6 +735,8 @@ std::vector<SchedOp> fuse_two_qubit_blocks(const std::vector<SchedOp>& ops, std:
       o.unit = unit;
       o.mat = (uint32_t)pool.size();
       for (int j = 0; j < d; ++j) pool.push_back({ph[2 * j], ph[2 * j + 1]});
+    } else if (b.k == 2) {
+      o.xpat = (uint8_t)classify_xpattern(flat);
     }
     out.push_back(o);
   }
@@ -865,6 +914,24 @@ struct Decomposer {
       const cplx64 dl = cm((col & 1) ? pb[q0] : pa[q0], (col & 2) ? pb[q1] : pa[q1]);
       Dp[r] = cm(ph[r], dl);
     }
+    bool unit_modulus = true;
+    for (int r = 0; r < 4; ++r) unit_modulus = unit_modulus && std::fabs(cabs2(ph[r]) - 1.0) < 1e-12;
+    if (!unit_modulus) {
+      // a non-unitary diagonal part (a channel's damping factors): carried on it
+      // would make the next gates on these qubits non-unitary, so it keeps its
+      // place with the pending diagonals folded into its phases
+      SchedOp o = src;
+      o.unit = 0;
+      o.urows = 0;
+      o.mat = put({Dp[0], Dp[1], Dp[2], Dp[3]});
+      o.dense = (uint32_t)pool.size();
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+          pool.push_back(((src.perm >> (2 * r)) & 3) == c ? Dp[r] : cplx64{0.0, 0.0});
+      pa[q0] = pa[q1] = pb[q0] = pb[q1] = {1.0, 0.0};
+      out.push_back(o);
+      return;
+    }
     const cplx64 s0 = Dp[0];
     const cplx64 x1 = cdiv(Dp[1], s0), y1 = cdiv(Dp[2], s0);
     const cplx64 gamma = cdiv(Dp[3], cm(s0, cm(x1, y1)));
@@ -897,6 +964,8 @@ struct Decomposer {
         pool.push_back(cm(pool[src.dense + r * d + c], f));
       }
     for (int j = 0; j < src.k; ++j) pa[src.q[j]] = pb[src.q[j]] = {1.0, 0.0};
+    if (src.xpat)   // the diagonal scales columns: same shape, entries maybe complex now
+      o.xpat = (uint8_t)classify_xpattern(reinterpret_cast<const double*>(pool.data() + o.dense));
     out.push_back(o);
   }
 };

@@ -321,6 +321,28 @@ __device__ __forceinline__ void m1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   }
 }
 
+// OP_X2R on slots A (bit 0) and B (bit 1); flags bit 0 / 1: corners / middle real
+template <int R, int A, int B>
+__device__ __forceinline__ void x2r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int flags) {
+  const double2 m0 = ld_mat(m, 0), m3 = ld_mat(m, 3), m12 = ld_mat(m, 12), m15 = ld_mat(m, 15), m5 = ld_mat(m, 5),
+                m10 = ld_mat(m, 10);
+#pragma unroll
+  for (int v = 0; v < (1 << R); ++v) {
+    if (v & ((1 << A) | (1 << B))) continue;
+    double2 x0 = s[v], x1 = s[v | (1 << A)], x2 = s[v | (1 << B)], x3 = s[v | (1 << A) | (1 << B)];
+    switch (flags & 3) {
+      case 3: xpat4<true, true>(x0, x1, x2, x3, m0, m3, m12, m15, m5, m10); break;
+      case 1: xpat4<true, false>(x0, x1, x2, x3, m0, m3, m12, m15, m5, m10); break;
+      case 2: xpat4<false, true>(x0, x1, x2, x3, m0, m3, m12, m15, m5, m10); break;
+      default: xpat4<false, false>(x0, x1, x2, x3, m0, m3, m12, m15, m5, m10); break;
+    }
+    d[v] = x0;
+    d[v | (1 << A)] = x1;
+    d[v | (1 << B)] = x2;
+    d[v | (1 << A) | (1 << B)] = x3;
+  }
+}
+
 template <int R, int B, int GEN, int FORM>
 __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
   const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u3 = ld_mat(m, 3);
@@ -467,6 +489,21 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
       else r1l<R, 0>(s, d, m, od.a, lane8, omask);
       break;
     case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
+    case OP_X2R:
+      switch (od.a * 8 + od.b) {
+#define IQ_X2R_CASE(A, B)                                               \
+  case A * 8 + B:                                                       \
+    if constexpr (A < R && B < R && A != B) x2r<R, A, B>(s, d, m, od.flags); \
+    break;
+        IQ_X2R_CASE(0, 1) IQ_X2R_CASE(0, 2) IQ_X2R_CASE(0, 3) IQ_X2R_CASE(0, 4)
+        IQ_X2R_CASE(1, 0) IQ_X2R_CASE(1, 2) IQ_X2R_CASE(1, 3) IQ_X2R_CASE(1, 4)
+        IQ_X2R_CASE(2, 0) IQ_X2R_CASE(2, 1) IQ_X2R_CASE(2, 3) IQ_X2R_CASE(2, 4)
+        IQ_X2R_CASE(3, 0) IQ_X2R_CASE(3, 1) IQ_X2R_CASE(3, 2) IQ_X2R_CASE(3, 4)
+        IQ_X2R_CASE(4, 0) IQ_X2R_CASE(4, 1) IQ_X2R_CASE(4, 2) IQ_X2R_CASE(4, 3)
+#undef IQ_X2R_CASE
+        default: break;
+      }
+      break;
     case OP_D2R:
       // one jump over the ordered slot pair (a, b) instead of nested compares
       switch (od.a * 8 + od.b) {

@@ -151,6 +151,23 @@ struct Emu {
             }
             break;
           }
+          case OP_X2R: {   // only the corners and the middle are read (their real parts when flagged)
+            auto ent = [&](int i, bool real) { const cd e = mat(od.mat, i); return real ? cd(e.real(), 0.0) : e; };
+            const bool cr = od.flags & 1, mr = od.flags & 2;
+            const cd m0 = ent(0, cr), m3 = ent(3, cr), m12 = ent(12, cr), m15 = ent(15, cr), m5 = ent(5, mr),
+                     m10 = ent(10, mr);
+            for (int L = 0; L < 8; ++L)
+              for (int v = 0; v < NV; ++v) {
+                if (v & ((1 << od.a) | (1 << od.b))) continue;
+                const int i0 = v, i1 = v | (1 << od.a), i2 = v | (1 << od.b), i3 = i1 | i2;
+                const cd x0 = a[L][i0], x3 = a[L][i3];
+                a[L][i0] = m0 * x0 + m3 * x3;
+                a[L][i3] = m12 * x0 + m15 * x3;
+                a[L][i1] *= m5;
+                a[L][i2] *= m10;
+              }
+            break;
+          }
           case OP_D2R:
           case OP_M2R:
             for (int L = 0; L < 8; ++L)
@@ -422,6 +439,8 @@ extern "C" int emu_apply(int nbits, int M, int c, int R, int max_stages, double 
       o.unit = unit;
       o.mat = (uint32_t)e.pool.size();
       for (int j = 0; j < d; ++j) e.pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    } else if (ks[i] == 2) {
+      o.xpat = (uint8_t)classify_xpattern(m);   // as the runtime's queue classifies it
     }
     ops.push_back(o);
   }
@@ -504,6 +523,8 @@ extern "C" int emu_jit_sources(int nbits, int M, int c, int R, int max_stages, d
       o.unit = unit;
       o.mat = (uint32_t)pool.size();
       for (int j = 0; j < d; ++j) pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    } else if (ks[i] == 2) {
+      o.xpat = (uint8_t)classify_xpattern(m);   // as the runtime's queue classifies it
     }
     ops.push_back(o);
   }
@@ -626,6 +647,8 @@ extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, dou
       o.unit = unit;
       o.mat = (uint32_t)pool.size();
       for (int j = 0; j < d; ++j) pool.emplace_back(ph[2 * j], ph[2 * j + 1]);
+    } else if (ks[i] == 2) {
+      o.xpat = (uint8_t)classify_xpattern(m);   // as the runtime's queue classifies it
     }
     ops.push_back(o);
   }
@@ -649,7 +672,7 @@ extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, dou
     snprintf(out, (size_t)outlen, "plan: %s", err.c_str());
     return -1;
   }
-  static const char* kind[] = {"-", "D1R", "D1L", "D2R", "DKR", "M1R", "M1L", "M2R", "G2", "N1R", "R1R", "R1L"};
+  static const char* kind[] = {"-", "D1R", "D1L", "D2R", "DKR", "M1R", "M1L", "M2R", "G2", "N1R", "R1R", "R1L", "X2R"};
   char buf[256];
   for (size_t pi = 0; pi < plans.size(); ++pi) {
     const PassDesc& d = plans[pi].desc;

@@ -144,3 +144,26 @@ def test_adjoint_kernels_compile(emu, narrow):
         rc, log, size = compile_nvrtc(lib, s)
         assert rc == 0, log[:3000]
         assert size > 0
+
+
+def test_channel_kernels_compile(emu):
+    """Passes of a noisy density-matrix circuit in the specialised style hold
+    X2R operations (xpat4 on real / complex corners and middle) that compile."""
+    from tests.test_scheduler_emulated import superop_lsb
+    from invariantq_b200.channels import build_kraus_channel
+    from invariantq_b200.gates import gate_matrix
+    lib = nvrtc_lib()
+    if lib is None:
+        pytest.skip("libnvrtc not available")
+    nq, rng = 8, np.random.default_rng(2)
+    dep = superop_lsb(build_kraus_channel("depolarizing", [1e-3]))
+    amp = superop_lsb(build_kraus_channel("amp_damping", [2e-3]))
+    ops = []
+    for q in range(nq):
+        U = gate_matrix("u3", list(rng.uniform(0, 2 * np.pi, 3)))
+        ops += [([nq + q], U), ([q], np.conj(U)), ([q, nq + q], dep), ([q, nq + q], amp)]
+    srcs = sources(emu, 2 * nq, ops, M=12, c=4, budget=160.0, fuse=2)
+    picked = [s for s in srcs if "xpat4<" in s]
+    assert picked
+    rc, log, size = compile_nvrtc(lib, max(picked, key=len))
+    assert rc == 0, log[:3000]

@@ -209,3 +209,75 @@ def test_brickwall_register_slots(port, emu, R):
     ref = oracle_apply(port, ref, n, ops)
     got, npasses, per = run_emu(emu, n, [to_lsb(*o) for o in ops], start, M=11, c=5, R=R)
     assert np.max(np.abs(got - ref)) < 1e-12
+
+
+def superop_lsb(kraus):
+    """sum_k K (x) conj(K) on the local bits (column bit, row bit): local index
+    bit 0 = the column qubit, bit 1 = the row qubit (the runtime's dm_kraus)."""
+    S = np.zeros((4, 4), np.complex128)
+    for K in kraus:
+        for ro in range(2):
+            for co in range(2):
+                for ri in range(2):
+                    for ci in range(2):
+                        S[ro * 2 + co, ri * 2 + ci] += K[ro, ri] * np.conj(K[co, ci])
+    return S
+
+
+def plan_kinds(emu, nbits, lsb_ops, M, c, fuse=2):
+    nops = len(lsb_ops)
+    ks = np.array([len(q) for q, _ in lsb_ops], dtype=np.int32)
+    qs = np.full((nops, 5), -1, dtype=np.int32)
+    offs = np.zeros(nops, dtype=np.int64)
+    pool, off = [], 0
+    for i, (q, U) in enumerate(lsb_ops):
+        qs[i, : len(q)] = q
+        offs[i] = off
+        pool.append(np.asarray(U, np.complex128).reshape(-1))
+        off += pool[-1].size
+    pool = np.concatenate(pool)
+    buf = ctypes.create_string_buffer(16 << 20)
+    rc = emu.emu_plan_dump(nbits, M, c, 4, 8, ctypes.c_double(160.0), fuse, nops,
+                           ks.ctypes.data_as(ctypes.c_void_p), qs.ctypes.data_as(ctypes.c_void_p),
+                           pool.ctypes.data_as(ctypes.c_void_p), offs.ctypes.data_as(ctypes.c_void_p),
+                           buf, ctypes.c_longlong(len(buf)))
+    assert rc > 0
+    return buf.value.decode()
+
+
+@pytest.mark.parametrize("nq,M,c,seed", [(6, 10, 4, 0), (7, 12, 4, 1), (8, 11, 5, 2)])
+def test_channel_superoperators_x_pattern(emu, nq, M, c, seed):
+    """A noisy density-matrix circuit as the runtime queues it (unitary U on the
+    row bit and conj(U) on the column bit, Kraus channels as superoperators on
+    the (column, row) bit pair, CX on row and column pairs), planned in the
+    specialised-kernel style: the channels' superoperators run as X2R
+    operations (only their corners and middle read), and the result equals the
+    dense matrices applied one by one (1e-12)."""
+    from invariantq_b200.channels import build_kraus_channel
+    from invariantq_b200.gates import gate_matrix
+    rng = np.random.default_rng(seed)
+    nb = 2 * nq
+    chans = [build_kraus_channel("depolarizing", [1e-3]), build_kraus_channel("amp_damping", [2e-3]),
+             build_kraus_channel("phase_damping", [1e-3]),
+             build_kraus_channel("thermal_relaxation", [100e-6, 80e-6, 50e-9])]
+    cx = gate_matrix("cx")
+    cx_lsb = cx[np.ix_([0, 2, 1, 3], [0, 2, 1, 3])]   # control on local bit 1
+    ops = []
+    for layer in range(4):
+        for q in range(nq):
+            U = gate_matrix("u3", list(rng.uniform(0, 2 * np.pi, 3)))
+            ops += [([nq + q], U), ([q], np.conj(U)), ([q, nq + q], superop_lsb(chans[0]))]
+        for q in range(layer % 2, nq - 1, 2):
+            ops += [([nq + q + 1, nq + q], cx_lsb), ([q + 1, q], cx_lsb)]
+            for qq in (q, q + 1):
+                ops += [([qq, nq + qq], superop_lsb(chans[1])), ([qq, nq + qq], superop_lsb(chans[2]))]
+        for q in range(nq):
+            ops.append(([q, nq + q], superop_lsb(chans[3])))
+    rho = rng.normal(size=1 << nb) + 1j * rng.normal(size=1 << nb)
+    want = rho.copy()
+    for qs, U in ops:
+        want = apply_lsb_numpy(want, nb, qs, U)
+    got, npasses, per = run_emu(emu, nb, ops, rho, M=M, c=c, budget=160.0, fuse=2)
+    assert np.max(np.abs(got - want)) < 1e-12 * max(1.0, np.max(np.abs(want)))
+    dump = plan_kinds(emu, nb, ops, M, c)
+    assert "X2R" in dump and "D2R" not in dump
