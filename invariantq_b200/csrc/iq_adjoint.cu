@@ -170,7 +170,7 @@ struct Shape {
 bool same_op(const SchedOp& a, const SchedOp& b) {
   if (a.k != b.k || a.mono != b.mono || a.perm != b.perm || a.unit != b.unit || a.mat != b.mat ||
       a.dense != b.dense || a.grad != b.grad || a.gen != b.gen || a.gidx != b.gidx || a.rot != b.rot ||
-      a.norm != b.norm || a.urows != b.urows)
+      a.norm != b.norm || a.urows != b.urows || a.xpat != b.xpat || a.realm != b.realm)
     return false;
   for (int i = 0; i < a.k; ++i)
     if (a.q[i] != b.q[i]) return false;
@@ -569,20 +569,19 @@ bool finish(Workspace& w, int k, std::string& err) {
 // every set's).  want_grad = false: forward and energy only.
 bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<size_t>& sets, std::vector<JobOps>& jo,
                  const Shape* fw, bool fw_cached, const Shape* bw, bool bw_cached, bool want_grad, Stats& st,
-                 std::string& err, std::chrono::steady_clock::time_point t0) {
+                 std::string& err) {
   const uint32_t S = (uint32_t)sets.size();
   const int ngrads = want_grad ? (int)jo[0].grad_param.size() : 0;
   // staging slot: wait for the job that used it last
   const int k = w.slot;
   w.slot ^= 1;
-  const auto tw = std::chrono::steady_clock::now();
   if (!finish(w, k, err)) return false;
-  const auto tw1 = std::chrono::steady_clock::now();
   const size_t nf = fw->gather.size(), nb = want_grad ? bw->gather.size() : 0;
   const size_t per = nf + nb;
   if (!w.hmats[k].ensure(per * S, err) || !w.hout[k].ensure(S + (size_t)S * ngrads, err) || !w.hstat[k].ensure(1, err))
     return false;
   double2* hm = w.hmats[k].p;
+  const auto tg = std::chrono::steady_clock::now();
   for (uint32_t j = 0; j < S; ++j) {
     const JobOps& o = jo[j];
     double2* f = hm + (size_t)j * nf;
@@ -590,6 +589,8 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
     double2* b = hm + (size_t)S * nf + (size_t)j * nb;
     for (size_t i = 0; i < nb; ++i) b[i] = make_double2(o.bpool[bw->gather[i]].re, o.bpool[bw->gather[i]].im);
   }
+  st.host_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - tg)
+                    .count();
   const uint64_t dim = 1ULL << c.n;
   const int nj = joint_bits(c.n);
   const uint64_t jdim = 1ULL << nj;
@@ -627,9 +628,6 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
   if (!cuda_ok(cudaMemcpyAsync(dm, hm, per * S * sizeof(double2), cudaMemcpyHostToDevice, w.stream), "H2D matrices",
                err))
     return false;
-  st.host_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                    (std::chrono::steady_clock::now() - t0) - (tw1 - tw))
-                    .count();
 
   double* partials = w.red.p;
   double* energy_dev = w.red.p + (size_t)S * kRedBlocks;
@@ -714,11 +712,19 @@ bool launch_sets(Workspace& w, const Cfg& cfg, Circuit& c, const std::vector<siz
 // any other set runs alone with plans of its own.
 bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set0, size_t nsets, bool want_grad, Stats& st,
                 std::string& err) {
-  const auto t0 = std::chrono::steady_clock::now();
+  // host preparation (st.host_ns): building the operation lists, planning a
+  // structure the first time, matching the sets against it and staging their
+  // matrices -- CPU work only, not the CUDA calls (which may wait for the stream)
+  auto since = [](std::chrono::steady_clock::time_point a) {
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - a).count();
+  };
+  auto t0 = std::chrono::steady_clock::now();
   std::vector<JobOps> jo(nsets);
   for (size_t j = 0; j < nsets; ++j) job_ops(cfg, c, c.params + (set0 + j) * (size_t)c.nparams, want_grad, jo[j]);
+  st.host_ns += since(t0);
   {
     std::lock_guard<std::mutex> g(c.mu);
+    t0 = std::chrono::steady_clock::now();
     if (!c.planned) {
       c.planned = true;
       c.fw.reset(new Shape);
@@ -729,11 +735,13 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set0, size_t ns
         else c.bw->ngrads = (int)jo[0].grad_param.size();
       }
     }
+    st.host_ns += since(t0);
     if (!c.fw || (want_grad && !c.bw)) {
       err = "scheduler: " + c.plan_err;
       return false;
     }
   }
+  t0 = std::chrono::steady_clock::now();
   std::vector<size_t> same, other;
   std::vector<JobOps> jsame;
   for (size_t j = 0; j < nsets; ++j) {
@@ -746,11 +754,11 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set0, size_t ns
       other.push_back(j);
     }
   }
-  if (!same.empty() &&
-      !launch_sets(w, cfg, c, same, jsame, c.fw.get(), true, c.bw.get(), true, want_grad, st, err, t0))
+  st.host_ns += since(t0);
+  if (!same.empty() && !launch_sets(w, cfg, c, same, jsame, c.fw.get(), true, c.bw.get(), true, want_grad, st, err))
     return false;
   for (size_t j : other) {   // a set whose angles change the fused structure
-    const auto t1 = std::chrono::steady_clock::now();
+    t0 = std::chrono::steady_clock::now();
     std::unique_ptr<Shape> own_fw(new Shape), own_bw;
     if (!make_shape(cfg, c.n, jo[j].fw, jo[j].fpool.size(), w.num_sms, *own_fw, err)) return false;
     if (want_grad) {
@@ -758,10 +766,11 @@ bool launch_job(Workspace& w, const Cfg& cfg, Circuit& c, size_t set0, size_t ns
       if (!make_shape(cfg, joint_bits(c.n), jo[j].bw, jo[j].bpool.size(), w.num_sms, *own_bw, err)) return false;
       own_bw->ngrads = (int)jo[j].grad_param.size();
     }
+    st.host_ns += since(t0);
     ++st.replans;
     std::vector<JobOps> one(1);
     one[0] = std::move(jo[j]);
-    if (!launch_sets(w, cfg, c, {set0 + j}, one, own_fw.get(), false, own_bw.get(), false, want_grad, st, err, t1))
+    if (!launch_sets(w, cfg, c, {set0 + j}, one, own_fw.get(), false, own_bw.get(), false, want_grad, st, err))
       return false;
   }
   return true;

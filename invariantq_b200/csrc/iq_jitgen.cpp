@@ -93,11 +93,17 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
     switch (od.kind) {
       case OP_D1R: {
         const int A = 1 << od.a;
+        const bool real = od.flags & OPF_REAL;
         for (int v = 0; v < NV; ++v) {
           if (v & A) continue;
           const std::string x = cur[v], y = cur[v | A];
-          cur[v] = def("cfma(cmul(" + mat(m + 0) + ", " + x + "), " + mat(m + 1) + ", " + y + ")");
-          cur[v | A] = def("cfma(cmul(" + mat(m + 2) + ", " + x + "), " + mat(m + 3) + ", " + y + ")");
+          if (real) {
+            cur[v] = def("rlin(" + mat(m + 0) + ".x, " + x + ", " + mat(m + 1) + ".x, " + y + ")");
+            cur[v | A] = def("rlin(" + mat(m + 2) + ".x, " + x + ", " + mat(m + 3) + ".x, " + y + ")");
+          } else {
+            cur[v] = def("cfma(cmul(" + mat(m + 0) + ", " + x + "), " + mat(m + 1) + ", " + y + ")");
+            cur[v | A] = def("cfma(cmul(" + mat(m + 2) + ", " + x + "), " + mat(m + 3) + ", " + y + ")");
+          }
         }
         break;
       }
@@ -160,7 +166,8 @@ bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int g
         o << "        const double2 " << co << " = " << hi << " ? " << mat(m + 2) << " : " << mat(m + 1) << ";\n";
         for (int v = 0; v < NV; ++v) {
           const std::string p = def("shfl_xor2(" + cur[v] + ", " + std::to_string(1 << l) + ", omask)");
-          cur[v] = def("cfma(cmul(" + cs + ", " + cur[v] + "), " + co + ", " + p + ")");
+          cur[v] = (od.flags & OPF_REAL) ? def("rlin(" + cs + ".x, " + cur[v] + ", " + co + ".x, " + p + ")")
+                                         : def("cfma(cmul(" + cs + ", " + cur[v] + "), " + co + ", " + p + ")");
         }
         break;
       }

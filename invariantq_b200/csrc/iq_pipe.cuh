@@ -165,6 +165,11 @@ __device__ __forceinline__ double2 rot_lane(double w, bool hi, double2 x, double
   return make_double2(fma(w, x.x, hi ? p.x : -p.x), fma(w, x.y, hi ? p.y : -p.y));
 }
 
+// a x + b y for real a, b (the rows of a real 2x2: OPF_REAL): 2 FP64 operations per component
+__device__ __forceinline__ double2 rlin(double a, double2 x, double b, double2 y) {
+  return make_double2(fma(b, y.x, a * x.x), fma(b, y.y, a * x.y));
+}
+
 // OP_X2R on one amplitude quadruple x0..x3 (local index bit 0 = slot a, bit 1
 // = slot b) with the 4x4 m (row-major): corners (0,0), (0,3), (3,0), (3,3) mix
 // x0 and x3, the middle (1,1), (2,2) scales x1 and x2.  CR / MR: the corner /

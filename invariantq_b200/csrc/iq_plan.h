@@ -95,6 +95,7 @@ constexpr uint8_t XPAT_MIDDLE_REAL = 4;
 
 // flags
 constexpr uint8_t OPF_UNIT_PHASE = 1;  // monomial whose phases are all exactly 1
+constexpr uint8_t OPF_REAL = 2;        // OP_D1R / OP_D1L whose entries are real (4 FMAs per amplitude, not 8)
 
 // Forms of an adjoint step's inverse rotation (OP_GRAD2 flags).  The step may
 // apply a multiple of the inverse: a unit phase common to psi and lambda
@@ -173,6 +174,7 @@ struct SchedOp {
   uint8_t urows;         // monomial: bit r = row r's phase is exactly 1
   uint8_t grad;          // 1: adjoint step (k = 2; q[0] = select bit, q[1] = qubit bit; 2x2 matrix)
   uint8_t xpat;          // k = 2 dense matrix of OP_X2R's shape: XPAT_* bits (0: not)
+  uint8_t realm;         // k = 1 dense matrix with real entries (OPF_REAL)
   uint8_t gen;           // adjoint step generator: 0 = X, 1 = Y, 2 = Z
   uint32_t gidx;         // adjoint step gradient term index (increasing in queue order)
   // factor the operation multiplies the scale of a scaled backward sweep by
@@ -429,8 +431,9 @@ struct AnsatzOp {
 // Validate an ansatz; returns the number of parameters it reads (max index + 1) or -1.
 int ansatz_check(int n, const std::vector<AnsatzOp>& ops, std::string& err);
 // Forward circuit on an n-bit state vector: ops appended to `out` (matrices to `pool`).
+// phase_free: RZ (and P) as diag(1, e^{i theta}), the global phase dropped.
 void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                    std::vector<cplx64>& pool);
+                    std::vector<cplx64>& pool, bool phase_free = false);
 // Backward sweep on the joint array of n + 1 bits (bit 0 selects psi (0) or
 // lambda = H psi (1), bit q + 1 is qubit q): for every gate from last to first,
 // an adjoint step (gradient term + inverse rotation) per rotation angle, or the

@@ -36,6 +36,7 @@ double op_cost(const SchedOp& op, double grad_cost) {
   }
   if (op.rot) return 2.0;
   if (op.norm) return 6.0;
+  if (op.realm && op.k == 1) return 4.0;
   if (op.xpat) return ((op.xpat & XPAT_CORNERS_REAL) ? 2.0 : 4.0) + ((op.xpat & XPAT_MIDDLE_REAL) ? 1.0 : 2.0);
   return 4.0 * double(1u << op.k);
 }
@@ -477,12 +478,14 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
           const int j = pos[o.q[0]];
           if (slot_of[j] >= 0) {
             od.kind = o.mono ? OP_M1R : (o.rot ? OP_R1R : (o.norm ? OP_N1R : OP_D1R));
+            if (od.kind == OP_D1R && o.realm) od.flags |= OPF_REAL;
             od.a = (uint8_t)slot_of[j];
             if (o.norm) od.perm = (uint8_t)(o.norm - 1);
             if (o.rot) od.perm = (uint8_t)(o.rot - 1);
           }
           else if (lane_of[j] >= 0) {
             od.kind = o.mono ? OP_M1L : (o.rot ? OP_R1L : OP_D1L);
+            if (od.kind == OP_D1L && o.realm && !o.norm) od.flags |= OPF_REAL;
             od.a = (uint8_t)lane_of[j];
             if (o.rot) od.perm = (uint8_t)(o.rot - 1);
           }
@@ -762,12 +765,14 @@ void normalize_one_qubit_ops(std::vector<SchedOp>& ops, std::vector<cplx64>& poo
       for (int e = 0; e < 4; ++e) pool.push_back(e == col ? cplx64{1.0, 0.0} : cm(pool[o.dense + e], inv));
       o.dense = o.mat = at;
       o.norm = (uint8_t)(col + 1);
+      o.realm = 0;
       scale = cm(scale, s);
     }
     SchedOp& c = ops[dense1[s1 - 1]];   // the run's carrier takes the product of the divisors
     const uint32_t at = (uint32_t)pool.size();
     for (int e = 0; e < 4; ++e) pool.push_back(cm(pool[c.dense + e], scale));
     c.dense = c.mat = at;
+    c.realm = 0;
   }
 }
 
@@ -899,6 +904,7 @@ struct Decomposer {
     o.dense = o.mat = put({A, B, C, D});
     o.norm = 0;
     o.rot = 0;
+    o.realm = 0;
     pa[q] = pb[q] = {1.0, 0.0};
     out.push_back(o);
   }
@@ -1031,7 +1037,14 @@ void push_op(std::vector<SchedOp>& out, std::vector<cplx64>& pool, int k, const 
     o.perm = perm;
     o.unit = unit;
     o.mat = (uint32_t)pool.size();
-    for (int i = 0; i < d; ++i) pool.push_back({ph[2 * i], ph[2 * i + 1]});
+    for (int i = 0; i < d; ++i) {
+      pool.push_back({ph[2 * i], ph[2 * i + 1]});
+      if (ph[2 * i] == 1.0 && ph[2 * i + 1] == 0.0) o.urows |= (uint8_t)(1u << i);   // its product is skipped
+    }
+  } else if (k == 1) {
+    bool real = true;
+    for (int i = 0; i < 4; ++i) real = real && flat[2 * i + 1] == 0.0;
+    o.realm = real ? 1 : 0;
   }
   out.push_back(o);
 }
@@ -1097,7 +1110,7 @@ int ansatz_check(int n, const std::vector<AnsatzOp>& ops, std::string& err) {
 }
 
 void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* params, std::vector<SchedOp>& out,
-                    std::vector<cplx64>& pool) {
+                    std::vector<cplx64>& pool, bool phase_free) {
   (void)n;
   for (const AnsatzOp& o : ops) {
     int gen[3], par[3];
@@ -1106,6 +1119,11 @@ void ansatz_forward(int n, const std::vector<AnsatzOp>& ops, const double* param
       for (int r = 0; r < nr; ++r) {
         cdd m[4];
         rotation(gen[r], params[par[r]], m);
+        if (phase_free && gen[r] == 2) {   // e^{-i th/2} diag(1, e^{i th}): the common phase dropped
+          const double th = params[par[r]];
+          m[0] = 1.0;
+          m[3] = cdd(std::cos(th), std::sin(th));
+        }
         const int q[1] = {o.q0};
         push_op(out, pool, 1, q, m);
       }
@@ -1199,13 +1217,25 @@ void adjoint_ops(int n, const std::vector<AnsatzOp>& ops, const double* params, 
                  bool single_set, AdjointOps& j) {
   j.fw.clear(); j.bw.clear(); j.fpool.clear(); j.bpool.clear(); j.grad_param.clear(); j.grad_scale.clear();
   std::vector<SchedOp> raw;
-  ansatz_forward(n, ops, params, raw, j.fpool);
+  // a global phase of psi changes neither the energy nor any Im<lambda|P|psi>
+  ansatz_forward(n, ops, params, raw, j.fpool, /*phase_free=*/!single_set);
   if (single_set) {
     j.fw = fuse_two_qubit_blocks(raw, j.fpool, true);
     decompose_one_qubit_ops(j.fw, j.fpool);
     normalize_one_qubit_ops(j.fw, j.fpool);
   } else {
-    j.fw = fuse ? fuse_two_qubit_blocks(raw, j.fpool) : raw;
+    // forms that do not depend on the angles, every gate alone: RY (and any
+    // real gate) a real 2x2 (4 FMAs per amplitude), RZ diag(1, e^{i th}) (2),
+    // CZ / CX renamings -- cheaper than fused 4x4 blocks (16); `fuse` = false
+    // keeps the plain matrices
+    j.fw = raw;
+    if (!fuse) {
+      raw.clear();
+      j.fpool.clear();
+      ansatz_forward(n, ops, params, raw, j.fpool, false);
+      for (SchedOp& o : raw) o.realm = 0;
+      j.fw = raw;
+    }
   }
   if (!backward) return;
   raw.clear();

@@ -57,14 +57,20 @@ inline cudaError_t allow_full_dynamic_smem(K kern, std::atomic<uint64_t>& done) 
 // (s and d alias); the INPLACE flag selects orders that stay correct then.
 
 template <int R, int S>
-__device__ __forceinline__ void d1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
+__device__ __forceinline__ void d1r(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
+                                    bool real = false) {
   const double2 u0 = ld_mat(m, 0), u1 = ld_mat(m, 1), u2 = ld_mat(m, 2), u3 = ld_mat(m, 3);
 #pragma unroll
   for (int v = 0; v < (1 << R); ++v) {
     if (v & (1 << S)) continue;
     const double2 x = s[v], y = s[v | (1 << S)];
-    d[v] = cfma(cmul(u0, x), u1, y);
-    d[v | (1 << S)] = cfma(cmul(u2, x), u3, y);
+    if (real) {   // OPF_REAL: the imaginary parts are zero and not read
+      d[v] = rlin(u0.x, x, u1.x, y);
+      d[v | (1 << S)] = rlin(u2.x, x, u3.x, y);
+    } else {
+      d[v] = cfma(cmul(u0, x), u1, y);
+      d[v | (1 << S)] = cfma(cmul(u2, x), u3, y);
+    }
   }
 }
 
@@ -282,7 +288,7 @@ __device__ __forceinline__ void dkr_store(const double2 (&a)[1 << R], const doub
 
 template <int R>
 __device__ __forceinline__ void d1l(const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m, int lb,
-                                    int lane8, unsigned omask) {
+                                    int lane8, unsigned omask, bool real = false) {
   const int my = (lane8 >> lb) & 1;
   const double2 cs = my ? ld_mat(m, 3) : ld_mat(m, 0);
   const double2 co = my ? ld_mat(m, 2) : ld_mat(m, 1);
@@ -290,7 +296,7 @@ __device__ __forceinline__ void d1l(const double2 (&s)[1 << R], double2 (&d)[1 <
   for (int v = 0; v < (1 << R); ++v) {
     const double2 x = s[v];
     const double2 p = shfl_xor2(x, 1 << lb, omask);
-    d[v] = cfma(cmul(cs, x), co, p);
+    d[v] = real ? rlin(cs.x, x, co.x, p) : cfma(cmul(cs, x), co, p);
   }
 }
 
@@ -361,10 +367,11 @@ __device__ __forceinline__ double grad2(const double2 (&s)[1 << R], double2 (&d)
 // ------------------------------------------------------- runtime dispatch
 
 template <int R, int S = 0>
-__device__ __forceinline__ void disp_d1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m) {
+__device__ __forceinline__ void disp_d1r(int sl, const double2 (&s)[1 << R], double2 (&d)[1 << R], const double2* m,
+                                         bool real) {
   if constexpr (S < R) {
-    if (sl == S) d1r<R, S>(s, d, m);
-    else disp_d1r<R, S + 1>(sl, s, d, m);
+    if (sl == S) d1r<R, S>(s, d, m, real);
+    else disp_d1r<R, S + 1>(sl, s, d, m, real);
   }
 }
 template <int R, int S = 0>
@@ -481,14 +488,14 @@ __device__ __forceinline__ bool apply_op(const OpDesc& od, const double2 (&s)[1 
       grad_accumulate(acc, sgrad + od.gidx, lane8, omask);
       break;
     }
-    case OP_D1R: disp_d1r<R>(od.a, s, d, m); break;
+    case OP_D1R: disp_d1r<R>(od.a, s, d, m, od.flags & OPF_REAL); break;
     case OP_N1R: disp_n1r<R>(od.a, od.perm, s, d, m); break;
     case OP_R1R: disp_r1r<R>(od.a, od.perm, s, d, m); break;
     case OP_R1L:
       if (od.perm) r1l<R, 1>(s, d, m, od.a, lane8, omask);
       else r1l<R, 0>(s, d, m, od.a, lane8, omask);
       break;
-    case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask); break;
+    case OP_D1L: d1l<R>(s, d, m, od.a, lane8, omask, od.flags & OPF_REAL); break;
     case OP_X2R:
       switch (od.a * 8 + od.b) {
 #define IQ_X2R_CASE(A, B)                                               \

@@ -109,23 +109,28 @@ struct Emu {
         switch (od.kind) {
           case OP_D1R:
           case OP_N1R:   // stored whole (its unit entry included)
-          case OP_R1R:
+          case OP_R1R: {
+            // OPF_REAL (dense kinds): only the real parts are read
+            const bool re = (od.flags & OPF_REAL) && od.kind == OP_D1R;
+            auto m1 = [&](int i) { const cd e = mat(od.mat, i); return re ? cd(e.real(), 0.0) : e; };
             for (int L = 0; L < 8; ++L)
               for (int v = 0; v < NV; ++v) {
                 if (v & (1 << od.a)) continue;
                 const cd x = a[L][v], y = a[L][v | (1 << od.a)];
-                a[L][v] = mat(od.mat, 0) * x + mat(od.mat, 1) * y;
-                a[L][v | (1 << od.a)] = mat(od.mat, 2) * x + mat(od.mat, 3) * y;
+                a[L][v] = m1(0) * x + m1(1) * y;
+                a[L][v | (1 << od.a)] = m1(2) * x + m1(3) * y;
               }
             break;
+          }
           case OP_D1L:
           case OP_R1L: {   // the rotation's matrix is stored whole
+            const bool re = (od.flags & OPF_REAL) && od.kind == OP_D1L;
+            auto m1 = [&](int i) { const cd e = mat(od.mat, i); return re ? cd(e.real(), 0.0) : e; };
             auto old = a;
             for (int L = 0; L < 8; ++L) {
               const int my = (L >> od.a) & 1, pl = L ^ (1 << od.a);
               for (int v = 0; v < NV; ++v)
-                a[L][v] = (my ? mat(od.mat, 3) : mat(od.mat, 0)) * old[L][v] +
-                          (my ? mat(od.mat, 2) : mat(od.mat, 1)) * old[pl][v];
+                a[L][v] = (my ? m1(3) : m1(0)) * old[L][v] + (my ? m1(2) : m1(1)) * old[pl][v];
             }
             break;
           }
