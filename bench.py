@@ -635,9 +635,12 @@ def adjoint30_section(args):
     rng = np.random.default_rng(30)
     th = rng.uniform(0, 2 * np.pi, a.num_params)
     adjoint_gradient(a, h, th)                     # warm-up: planning, workspace
-    t0 = time.perf_counter()
-    e, g = adjoint_gradient(a, h, th)
-    t = time.perf_counter() - t0
+    times = []
+    for _ in range(3):                             # median of 3 timed gradients
+        t0 = time.perf_counter()
+        e, g = adjoint_gradient(a, h, th)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
     st = adjoint_stats()
     idx = rng.choice(a.num_params, 4, replace=False)
     sets = shifted_parameter_sets(th)
@@ -647,17 +650,22 @@ def adjoint30_section(args):
     from invariantq_b200.gradients import adjoint_gradient_c64, adjoint_release
     adjoint_release()                              # the complex128 workspace
     adjoint_gradient_c64(a, h, th)                 # warm-up: its kernels and workspace
-    t0 = time.perf_counter()
-    e32, g32 = adjoint_gradient_c64(a, h, th)
-    t32 = time.perf_counter() - t0
+    times32 = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        e32, g32 = adjoint_gradient_c64(a, h, th)
+        times32.append(time.perf_counter() - t0)
+    t32 = float(np.median(times32))
     adjoint_release()
     return {"workload": f"{n}q, {L} layers RY+RZ per qubit + CZ ring ({a.num_params} parameters), TFIM h=0.7, complex128; "
                         "state memory: one [psi | lambda] array of 2^(n+1) amplitudes (two state-sized buffers)",
-            "gradient_s": round(t, 3), "energy": e, "passes": {"forward": int(st["forward_passes"]),
+            "gradient_s": round(t, 3), "gradient_s_runs": [round(x, 3) for x in times], "timing": "median of 3 after a warm-up",
+            "energy": e, "passes": {"forward": int(st["forward_passes"]),
                                                               "backward": int(st["backward_passes"])},
             "achieved_gbs": round(st["bytes"] / t / 1e9, 1),
             "max_abs_diff_vs_param_shift": float(np.max(np.abs(ps - g[idx]))), "checked_parameters": [int(i) for i in idx],
-            "complex64": {"gradient_s": round(t32, 3), "energy_abs_err": abs(e32 - e),
+            "complex64": {"gradient_s": round(t32, 3), "gradient_s_runs": [round(x, 3) for x in times32],
+                          "energy_abs_err": abs(e32 - e),
                           "grad_max_abs_err": float(np.max(np.abs(g32 - g))),
                           "grad_rel_err": float(np.max(np.abs(g32 - g)) / max(np.max(np.abs(g)), 1e-300)),
                           "speedup_vs_complex128": round(t / t32, 3),
