@@ -315,6 +315,11 @@ class AdjointAutotuner:
             cid = adjoint_choice_id(cand)
             if cid not in times:
                 try:
+                    if not times:
+                        # the process's first batches also grow the workers' buffers to
+                        # their sizes: one more untimed run, so the first candidate is not
+                        # charged for it
+                        self.timer(sample, cand)
                     ms = float(self.timer(sample, cand))
                 except (ValueError, RuntimeError, MemoryError):
                     ms = float("inf")
