@@ -119,6 +119,35 @@ def test_density_matrix_specialised(B):
     del rng
 
 
+def test_density_matrix_channel_superoperators(B):
+    """Depolarizing, amplitude / phase damping and thermal relaxation channels
+    (superoperators of the corner + middle shape, run as X2R operations):
+    specialised and interpreting kernels give identical matrices; trace 1."""
+    from invariantq_b200.channels import build_kraus_channel
+    n = 8
+    chans = [build_kraus_channel("depolarizing", [2e-2]), build_kraus_channel("amp_damping", [3e-2]),
+             build_kraus_channel("phase_damping", [2e-2]),
+             build_kraus_channel("thermal_relaxation", [100e-6, 80e-6, 50e-9])]
+    mats = []
+    for jit in (0, 2):
+        dm = B.NativeDensityMatrix(n)
+        dm.set_option("jit", jit)
+        dm.set_option("plan_style", 2)
+        r = np.random.default_rng(8)
+        for _ in range(30):
+            a, b = (int(x) for x in r.choice(n, 2, replace=False))
+            dm.apply_1q_unitary(a, rand_unitary(r, 2))
+            dm.apply_1q_kraus(a, chans[int(r.integers(4))])
+            dm.apply_2q_unitary(a, b, np.eye(4)[[0, 1, 3, 2]])
+            dm.apply_1q_kraus(b, chans[int(r.integers(4))])
+            dm.apply_1q_kraus(b, chans[int(r.integers(4))])
+        mats.append(dm.get_matrix())
+        assert (dm.stats()["jit_passes"] > 0) == (jit == 2)
+        dm.close()
+    assert np.array_equal(mats[0], mats[1])
+    assert abs(np.trace(mats[1]).real - 1.0) < 1e-12
+
+
 def test_normalised_planning_vs_oracle(B, port):
     """Plan style 2 on the interpreting kernel, more dense one-qubit gates than
     one normalisation run (a CZ after each keeps them from merging)."""
