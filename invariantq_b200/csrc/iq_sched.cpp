@@ -98,6 +98,7 @@ struct PassBuilder {
   const SchedParams& p;
   int c;
   std::vector<Stage> stages;
+  bool allow_new = true;   // false: an operation joins the current stage or waits
   explicit PassBuilder(const SchedParams& pp, int cc) : p(pp), c(cc) {}
 
   static bool inS(const Stage& s, int b) {
@@ -200,7 +201,7 @@ struct PassBuilder {
           return true;
         }
       }
-      if ((int)stages.size() >= p.max_stages) return false;
+      if ((int)stages.size() >= p.max_stages || (!allow_new && !stages.empty())) return false;
       Stage s;
       s.S[s.nS++] = op.q[0];
       if (!tryAdd(s, op)) return false;
@@ -210,7 +211,7 @@ struct PassBuilder {
     }
     if (op.k >= 3) {
       if (op.k > p.R) return false;
-      if ((int)stages.size() >= p.max_stages) return false;
+      if ((int)stages.size() >= p.max_stages || (!allow_new && !stages.empty())) return false;
       Stage s;
       s.dk = true;
       for (int i = 0; i < op.k; ++i) s.S[s.nS++] = op.q[i];
@@ -226,7 +227,7 @@ struct PassBuilder {
         return true;
       }
     }
-    if ((int)stages.size() >= p.max_stages) return false;
+    if ((int)stages.size() >= p.max_stages || (!allow_new && !stages.empty())) return false;
     Stage s;
     if (!tryAdd(s, op)) return false;
     s.ops.push_back(idx);
@@ -363,28 +364,35 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
     int mat_elems = 0;
     int ngrad = 0;
     for (;;) {
+      // every ready operation that fits the current stage joins it before an
+      // operation may open the next stage
       bool progress = true;
       while (progress) {
         progress = false;
-        for (auto it = ready.begin(); it != ready.end();) {
-          const int i = *it;
-          const SchedOp& o = ops[i];
-          const double oc = op_cost(o, p.grad_cost);
-          if ((opmask(o) & ~local) == 0 && (int)taken.size() < kMaxPassOps &&
-              mat_elems + op_mat_elems(o) <= kSmemMatElems && (taken.empty() || cost + oc <= p.budget) &&
-              (!o.grad || ngrad < kMaxPassGrads) && pb.place(i, o)) {
-            taken.push_back(i);
-            cost += oc;
-            mat_elems += op_mat_elems(o);
-            ngrad += o.grad ? 1 : 0;
-            it = ready.erase(it);
-            retire(i);
-            progress = true;
-          } else {
-            ++it;
+        for (int phase = 0; phase < 2 && !progress; ++phase) {
+          pb.allow_new = phase == 1;
+          for (auto it = ready.begin(); it != ready.end();) {
+            const int i = *it;
+            const SchedOp& o = ops[i];
+            const double oc = op_cost(o, p.grad_cost);
+            if ((opmask(o) & ~local) == 0 && (int)taken.size() < kMaxPassOps &&
+                mat_elems + op_mat_elems(o) <= kSmemMatElems && (taken.empty() || cost + oc <= p.budget) &&
+                (!o.grad || ngrad < kMaxPassGrads) && pb.place(i, o)) {
+              taken.push_back(i);
+              cost += oc;
+              mat_elems += op_mat_elems(o);
+              ngrad += o.grad ? 1 : 0;
+              it = ready.erase(it);
+              retire(i);
+              progress = true;
+              if (phase == 1) break;   // one operation opens the stage; the others try to join it
+            } else {
+              ++it;
+            }
           }
         }
       }
+      pb.allow_new = true;
       if (free_slots == 0 || (int)taken.size() >= kMaxPassOps) break;
       int best = -1, bestmiss = 0;
       for (int i : ready) {
