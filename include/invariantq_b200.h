@@ -276,8 +276,10 @@ int iq_adjoint_gradient(size_t num_qubits, size_t num_ops, const int* kinds, con
                         const double* coeffs, const char* paulis, double* energy_out, double* grad_out);
 /* The same gradient with the states stored as complex64 (8 B per amplitude,
  * half the memory and traffic of complex128): every gate and Hamiltonian
- * product is computed in FP64 from the loaded amplitudes and rounded once on
- * store, every sum (gradient terms, energy) is accumulated in FP64.  One
+ * product is computed in FP64 from the loaded amplitudes, values are rounded
+ * to complex64 where they are stored (the array, and the shared-memory tile
+ * between register stages), every sum (gradient terms, energy) is
+ * accumulated in FP64.  One
  * parameter set; two state buffers (psi and lambda, 8 B x 2^n each).  The
  * result differs from iq_adjoint_gradient by the complex64 rounding of the
  * states (~1e-7 relative at 30 qubits, 16 layers). */

@@ -68,7 +68,7 @@ struct Cfg {
   int fuse = 1;
   int jit = 1;   // specialised kernels (iq_jit.cpp) for the forward and backward passes
   // complex64 states: every pass a specialised kernel that widens the loaded
-  // amplitudes to FP64 and rounds once on store (jit_launch_narrow)
+  // amplitudes to FP64 and rounds to FP32 at its stage boundaries (jit_launch_narrow)
   bool c64 = false;
   // a circuit with one parameter set: forward and backward in the forms that
   // depend on its angles (fewer FP64 operations; adjoint_ops' single_set)

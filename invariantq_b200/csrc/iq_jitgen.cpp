@@ -29,7 +29,7 @@ std::string mat(uint32_t i) { return (g_set_mode ? "smat[" : "Mt.m[") + std::to_
 // gmode bit 0: the stage loads its registers from the complex64 array in
 // global memory (gst + tile base tb + physical offsets) instead of the tile;
 // bit 1: it stores them there; bit 2: the shared-memory tile is complex64
-// (float2 `ftile`: values widened to FP64 on load, rounded once on store).
+// (float2 `ftile`: values widened to FP64 on load, rounded on store).
 bool gen_stage(Gen& g, const PassDesc& d, int s, int NT, std::string& err, int gmode = 0) {
   const StageDesc& sd = d.st[s];
   const int R = d.R, NV = 1 << R;

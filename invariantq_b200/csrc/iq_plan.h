@@ -374,8 +374,9 @@ int plan_passes(const SchedParams& p, const std::vector<SchedOp>& ops, std::vect
 // interpreting kernel's launch arguments); otherwise matrices are a kernel
 // parameter block.  narrow (with set_mode): the array is complex64 (float2);
 // the first stage loads from and the last stores to global memory directly,
-// widening to FP64 and rounding once (arguments: pass, matrices, state,
-// gradient partials; launched with jit_launch_narrow).
+// widening to FP64, and the stages exchange through a float2 shared tile
+// (arguments: pass, matrices, state, gradient partials; launched with
+// jit_launch_narrow).
 std::string jit_pass_source(const PassDesc& d, std::string& err, int min_blocks = 2, int threads = 0,
                             bool set_mode = false, bool narrow = false);
 // Compact byte string of everything jit_pass_source's output depends on
