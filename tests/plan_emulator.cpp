@@ -719,3 +719,38 @@ extern "C" int emu_plan_dump(int nbits, int M, int c, int R, int max_stages, dou
   memcpy(out, all.c_str(), all.size() + 1);
   return (int)plans.size();
 }
+
+// OP_X2R's shape classification (classify_xpattern) of a 4x4 row-major matrix
+// given as interleaved re/im doubles.
+extern "C" int emu_classify_xpattern(const double* m) { return classify_xpattern(m); }
+
+// Scales of a backward sweep's gradient terms in the order its planned passes
+// run the operations (exec_grad_scales), for an ansatz planned as the adjoint
+// executor plans a single-set circuit; also the queue-order scales
+// ansatz_backward reports.  Returns the number of terms (-1: error).
+extern "C" int emu_grad_scales(int n, int nops, const int* kinds, const int* q0, const int* q1, const int* pidx,
+                               const double* params, int M, int c, double* exec_scale, double* queue_scale, int cap) {
+  std::vector<AnsatzOp> ops(nops);
+  for (int i = 0; i < nops; ++i) ops[i] = {kinds[i], q0[i], q1[i], pidx[i]};
+  std::string err;
+  if (ansatz_check(n, ops, err) < 0) return -1;
+  AdjointOps jo;
+  adjoint_ops(n, ops, params, true, true, true, jo);
+  SchedParams p{};
+  p.nbits = std::max(n + 1, 7);
+  p.M = M;
+  p.c = c;
+  p.R = 4;
+  p.max_stages = 8;
+  p.budget = 200.0;
+  std::vector<PassPlan> plans;
+  if (plan_passes(p, jo.bw, plans, err) < 0) return -1;
+  std::vector<double> sc;
+  exec_grad_scales(&plans, jo.bw, sc);
+  if ((int)sc.size() > cap || sc.size() != jo.grad_scale.size()) return -1;
+  for (size_t t = 0; t < sc.size(); ++t) {
+    exec_scale[t] = sc[t];
+    queue_scale[t] = jo.grad_scale[t];
+  }
+  return (int)sc.size();
+}
