@@ -148,6 +148,32 @@ def test_density_matrix_channel_superoperators(B):
     assert abs(np.trace(mats[1]).real - 1.0) < 1e-12
 
 
+def test_x_shaped_two_qubit_gates(B, port):
+    """Two-qubit gates whose only nonzero entries are the corners
+    {00, 11} x {00, 11} and the middle diagonal, with complex entries (a
+    unitary on the {00, 11} pair and phases on 01, 10): they run as X2R with
+    complex corners and middle; specialised and interpreting kernels agree bit
+    for bit, and the oracle within 1e-12."""
+    n = 12
+    r = np.random.default_rng(21)
+    ops = []
+    for _ in range(40):
+        a, b = (int(x) for x in r.choice(n, 2, replace=False))
+        ops.append(("1q", [a], rand_unitary(r, 2)))
+        W = rand_unitary(r, 2)
+        X = np.zeros((4, 4), np.complex128)
+        X[np.ix_([0, 3], [0, 3])] = W
+        X[1, 1], X[2, 2] = np.exp(1j * r.uniform(0, 2 * np.pi, 2))
+        ops.append(("2q", [a, b], X))
+    opts = {"plan_style": 2}
+    a0, _ = run_sv(B, n, ops, 0, **opts)
+    a2, s2 = run_sv(B, n, ops, 2, **opts)
+    assert s2["jit_passes"] == s2["tile_passes"] > 0
+    assert np.array_equal(a0, a2)
+    ref = oracle_apply(port, port.zero_state(n), n, ops)
+    assert np.max(np.abs(a2 - ref)) < TOL
+
+
 def test_normalised_planning_vs_oracle(B, port):
     """Plan style 2 on the interpreting kernel, more dense one-qubit gates than
     one normalisation run (a CZ after each keeps them from merging)."""
